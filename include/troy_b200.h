@@ -1,0 +1,182 @@
+/*
+ * troy_b200.h - C ABI of the B200 ciphertext-arithmetic library.
+ *
+ * Plain C: opaque handles, raw device pointers, sizes and a cudaStream_t passed as
+ * `void *` (NULL = the legacy default stream). Every function returns a status
+ * (TB_OK = 0); tb_last_error() gives the message of the calling thread's last
+ * failure. Polynomials are uint64 words laid out [poly][limb][N] as in the
+ * reference (src/kernelutils.cu:41); limb l of a level-L ciphertext is modulus
+ * chain[l]. Pointers must be 16-byte aligned device memory.
+ *
+ * Each entry point names the reference interface it replaces. Paths are relative
+ * to the reference project (SecretHQ/seal-cuda).
+ */
+#ifndef TROY_B200_H
+#define TROY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TB_OK = 0,
+    TB_ERR_INVALID_ARGUMENT = 1,
+    TB_ERR_UNSUPPORTED = 2,
+    TB_ERR_CUDA = 3,
+    TB_ERR_OUT_OF_MEMORY = 4,
+    TB_ERR_NO_KEY = 5,
+    TB_ERR_TIMEOUT = 6
+};
+
+enum { TB_SCHEME_RAW = 0, TB_SCHEME_BFV = 1, TB_SCHEME_CKKS = 2, TB_SCHEME_BGV = 3 };
+
+typedef struct tb_context tb_context;
+
+/* Message of the calling thread's most recent error ("" if none). */
+const char *tb_last_error(void);
+
+/* ------------------------------------------------------------------ context */
+
+/*
+ * Creates the device-resident precompute for one parameter set: ring degree n,
+ * the key-level coefficient modulus chain (special prime last) and, for BFV/BGV,
+ * the plain modulus. Uploads NTT tables for every chain prime, the plain modulus
+ * (when 1 mod 2n) and the 61-bit Bsk primes, plus the RNS-tool constants of every
+ * chain level. Replaces SEALContextCuda construction with its NTTTablesCuda /
+ * RNSToolCuda uploads (src/context_cuda.cuh:28-61, src/utils/rns_cuda.cuh:76-141).
+ * scheme TB_SCHEME_RAW creates tables only (raw transforms).
+ */
+int tb_context_create(int scheme, uint64_t poly_degree, const uint64_t *coeff_moduli, int count,
+                      uint64_t plain_modulus, tb_context **out);
+int tb_context_destroy(tb_context *ctx);
+
+/* Moduli with NTT tables, in table order: chain, then t (if batching), then Bsk primes. */
+int tb_context_moduli(const tb_context *ctx, uint64_t *out, int capacity, int *count);
+
+/* ------------------------------------------------------------------ transforms */
+
+/*
+ * Negacyclic forward NTT of [polys][limbs][n]; limb l uses table modulus first+l.
+ * Bit-reversed output, lazy != 0 keeps values in [0, 4q) exactly as
+ * nttNegacyclicHarveyLazy. in may equal out.
+ * Replaces kernel_util::kNttNegacyclicHarvey[Lazy] (src/kernelutils.cuh:578-603).
+ */
+int tb_ntt_forward(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs,
+                   int lazy, void *stream);
+
+/*
+ * Inverse negacyclic NTT (bit-reversed in, natural out, N^-1 folded in); lazy != 0
+ * keeps values in [0, 2q). Replaces kernel_util::kInverseNttNegacyclicHarvey[Lazy]
+ * (src/kernelutils.cuh:607-632).
+ */
+int tb_ntt_inverse(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs,
+                   int lazy, void *stream);
+
+/* ------------------------------------------------------------- element-wise */
+
+/*
+ * out = a * b mod q per limb over [polys][limbs][n]. Replaces
+ * kernel_util::kDyadicProductCoeffmod (src/kernelutils.cuh:480-503).
+ */
+int tb_dyadic_product(tb_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t polys,
+                      int first, int limbs, void *stream);
+
+/*
+ * Ciphertext tensor product of B pairs of size-2 ciphertexts in the NTT domain:
+ * out = (a0 b0, a0 b1 + a1 b0, a1 b1), limbs first..first+L-1. Strides are words
+ * between consecutive ciphertexts (0 = packed: 2*L*n in, 3*L*n out); out must not
+ * overlap the inputs. This is the CKKS multiply (and the BGV multiply between its
+ * transforms). Replaces EvaluatorCuda::ckksMultiply's gDyadicConvolutionCoeffmod
+ * launches (src/evaluator_cuda.cu:384-432, src/kernelutils.cu:89).
+ */
+int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+                      uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+
+/*
+ * Multiplies `batch` pairs of size-2 ciphertexts at level L into size-3 outputs with
+ * the context's scheme: BFV by the BEHZ RNS method (EvaluatorCuda::bfvMultiply,
+ * src/evaluator_cuda.cu:283-382, over RNSToolCuda::fastbconvmTilde / smMrq /
+ * fastFloor / fastbconvSk, src/utils/rns_cuda.cu:339-443), BGV by NTT-tensor-INTT
+ * (src/evaluator_cuda.cu:435-501), CKKS by the NTT-domain tensor
+ * (src/evaluator_cuda.cu:384-432). Strides 0 = packed (2*L*n in, 3*L*n out); out must
+ * not overlap the inputs. BFV needs L <= 32.
+ */
+int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b, uint64_t b_stride,
+                uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+
+/* ------------------------------------------------------------ key switching */
+
+/*
+ * Key-switching key layout: the key-level KSwitchKeys entry of one key, as the
+ * reference stores it: [K-1 digits][2 polys][K limbs][n] words in NTT form, K =
+ * chain length (src/keygenerator.cpp:294-329, src/kswitchkeys_cuda.cuh:43-56).
+ *
+ * tb_keyswitch: for each of `batch` ciphertexts at level L (L data limbs, 1 <= L <= K-1)
+ * adds switch(target) into the ciphertext's first two polynomials. target[b] has L
+ * limbs at target + b*target_stride (NTT form for CKKS, coefficient form for
+ * BFV/BGV); ciphertext b at ct + b*ct_stride. Strides in words, 0 = packed.
+ * Replaces EvaluatorCuda::switchKeyInplace (src/evaluator_cuda.cu:1164-1363).
+ */
+int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target_stride, uint64_t *ct,
+                 uint64_t ct_stride, const uint64_t *key, uint64_t batch, void *stream);
+
+/*
+ * Relinearizes `batch` size-3 ciphertexts [b][3][L][n] in place (the first two
+ * polynomials receive the result; the third is left as is). ct_stride 0 = 3*L*n.
+ * key is the RelinKeys entry for s^2. Replaces EvaluatorCuda::relinearizeInternal
+ * (src/evaluator_cuda.cu:703-744).
+ */
+int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key, uint64_t batch,
+                   void *stream);
+
+/*
+ * Applies the Galois automorphism `galois_elt` to `batch` size-2 ciphertexts and
+ * key-switches with that element's Galois key: coefficient-domain permutation for
+ * BFV/BGV, NTT-domain permutation for CKKS. in may equal out. Replaces
+ * EvaluatorCuda::applyGaloisInplace (src/evaluator_cuda.cu:2011-2104) with
+ * GaloisToolCuda::applyGalois[Ntt] (src/utils/galois_cuda.cuh:21-25).
+ */
+int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t *in, uint64_t in_stride,
+                    uint64_t *out, uint64_t out_stride, const uint64_t *key, uint64_t batch, void *stream);
+
+/* Galois element of a rotation step (0 = column swap). Replaces GaloisTool::getEltFromStep
+   (src/utils/galois.cpp:45-88). */
+int tb_galois_elt_from_step(const tb_context *ctx, int step, uint32_t *elt);
+
+/* ------------------------------------------------------ rescale / mod switch */
+
+/*
+ * Divides `batch` ciphertexts of `size` polynomials at level L by the last prime
+ * with rounding and drops it (L limbs in, L-1 out): CKKS rescale in the NTT domain
+ * (RNSTool::divideAndRoundqLastNttInplace, src/utils/rns.cpp:831), BFV modulus
+ * switch (divideAndRoundqLastInplace, :805), BGV modulus switch
+ * (modTAndDivideqLastInplace, :1097). Ciphertext b at in + b*in_stride, its
+ * polynomials L*n words apart (out: (L-1)*n); strides 0 = packed. in and out must
+ * not overlap. Replaces EvaluatorCuda::modSwitchScaleToNext (src/evaluator_cuda.cu:749-824).
+ */
+int tb_rescale_to_next(tb_context *ctx, int L, const uint64_t *in, uint64_t in_stride, uint64_t *out,
+                       uint64_t out_stride, int size, uint64_t batch, void *stream);
+
+/* ---------------------------------------------------------------- tracing */
+
+/* Per-kernel device time of the library's launches (CUDA events on each launch's
+   stream). The reference has no tracing (its timers are host gettimeofday,
+   test/timetest.cu:16-57); this is new. */
+typedef struct {
+    char name[32];
+    uint64_t launches;
+    double total_ms;
+} tb_trace_entry;
+
+/* Starts (on != 0) or stops recording; either way drops what was recorded. */
+int tb_trace_enable(int on);
+/* Waits for the recorded launches and returns per-name totals; clears the record. */
+int tb_trace_collect(tb_trace_entry *out, int capacity, int *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,168 @@
+// The extern "C" boundary (include/troy_b200.h): argument checks, device selection
+// and status conversion around the internal launchers.
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "../../include/troy_b200.h"
+#include "context.hpp"
+
+namespace tb {
+extern thread_local std::string g_last_error;
+int dyadic_product(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t polys, int first,
+                   int limbs, cudaStream_t s);
+int tensor_product(const Context &c, int first, int L, const uint64_t *a, uint64_t astride, const uint64_t *b,
+                   uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const uint64_t *b, uint64_t bstride,
+             uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct, uint64_t cstride,
+              const uint64_t *key, uint64_t B, cudaStream_t s);
+int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
+                 uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s);
+int galois_elt_from_step(const Context &c, int step, uint32_t *elt);
+void trace_enable(bool on);
+int trace_collect(std::map<std::string, std::pair<uint64_t, double>> &out);
+int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, uint64_t *out, uint64_t cstride_out,
+                    int size, uint64_t B, cudaStream_t s);
+}  // namespace tb
+
+struct tb_context {
+    tb::Context *c;
+};
+
+using tb::set_error;
+
+namespace {
+// Runs f with the context's device current; restores the caller's device.
+template <class F>
+int on_device(const tb_context *ctx, F &&f) {
+    if (!ctx || !ctx->c) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null context");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->c->device) cudaSetDevice(ctx->c->device);
+    int st = f(*ctx->c);
+    if (prev != ctx->c->device && prev >= 0) cudaSetDevice(prev);
+    return st;
+}
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+const char *tb_last_error(void) { return tb::g_last_error.c_str(); }
+
+int tb_context_create(int scheme, uint64_t poly_degree, const uint64_t *coeff_moduli, int count,
+                      uint64_t plain_modulus, tb_context **out) {
+    if (!out) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    tb::Context *c = nullptr;
+    int st = tb::context_create(scheme, poly_degree, coeff_moduli, count, plain_modulus, &c);
+    if (st != TB_OK) return st;
+    *out = new tb_context{c};
+    return TB_OK;
+}
+
+int tb_context_destroy(tb_context *ctx) {
+    if (!ctx) return TB_OK;
+    delete ctx->c;
+    delete ctx;
+    return TB_OK;
+}
+
+int tb_context_moduli(const tb_context *ctx, uint64_t *out, int capacity, int *count) {
+    if (!ctx || !ctx->c || !count) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null argument");
+    const auto &m = ctx->c->table_moduli;
+    *count = (int)m.size();
+    if (out) std::memcpy(out, m.data(), sizeof(uint64_t) * std::min<size_t>(m.size(), capacity > 0 ? capacity : 0));
+    return TB_OK;
+}
+
+int tb_ntt_forward(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, int lazy,
+                   void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::ntt_forward(c, in, out, polys, first, limbs, lazy != 0, S(stream)); });
+}
+
+int tb_ntt_inverse(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, int lazy,
+                   void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::ntt_inverse(c, in, out, polys, first, limbs, lazy != 0, S(stream)); });
+}
+
+int tb_dyadic_product(tb_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t polys, int first,
+                      int limbs, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::dyadic_product(c, a, b, out, polys, first, limbs, S(stream)); });
+}
+
+int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+                      uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::tensor_product(c, first, L, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b, uint64_t b_stride,
+                uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::multiply(c, L, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target_stride, uint64_t *ct,
+                 uint64_t ct_stride, const uint64_t *key, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::keyswitch(c, L, target, target_stride, ct, ct_stride, key, batch, S(stream));
+    });
+}
+
+int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key, uint64_t batch,
+                   void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        const uint64_t stride = ct_stride ? ct_stride : 3ull * L * c.n;
+        if (!ct) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
+        return tb::keyswitch(c, L, ct + 2ull * L * c.n, stride, ct, stride, key, batch, S(stream));
+    });
+}
+
+int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t *in, uint64_t in_stride,
+                    uint64_t *out, uint64_t out_stride, const uint64_t *key, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::apply_galois(c, L, galois_elt, in, in_stride, out, out_stride, key, batch, S(stream));
+    });
+}
+
+int tb_galois_elt_from_step(const tb_context *ctx, int step, uint32_t *elt) {
+    if (!ctx || !ctx->c || !elt) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null argument");
+    return tb::galois_elt_from_step(*ctx->c, step, elt);
+}
+
+int tb_rescale_to_next(tb_context *ctx, int L, const uint64_t *in, uint64_t in_stride, uint64_t *out,
+                       uint64_t out_stride, int size, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::rescale_to_next(c, L, in, in_stride, out, out_stride, size, batch, S(stream));
+    });
+}
+
+int tb_trace_enable(int on) {
+    tb::trace_enable(on != 0);
+    return TB_OK;
+}
+
+int tb_trace_collect(tb_trace_entry *out, int capacity, int *count) {
+    if (!count) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null count");
+    std::map<std::string, std::pair<uint64_t, double>> m;
+    int st = tb::trace_collect(m);
+    if (st != TB_OK) return st;
+    int k = 0;
+    for (auto &kv : m) {
+        if (out && k < capacity) {
+            std::memset(out[k].name, 0, sizeof(out[k].name));
+            std::strncpy(out[k].name, kv.first.c_str(), sizeof(out[k].name) - 1);
+            out[k].launches = kv.second.first;
+            out[k].total_ms = kv.second.second;
+        }
+        k++;
+    }
+    *count = k;
+    return TB_OK;
+}
+
+}  // extern "C"

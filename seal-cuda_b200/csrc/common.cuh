@@ -1,0 +1,91 @@
+// Shared device definitions: the per-modulus descriptor kept in HBM and the exact
+// 64-bit modular arithmetic every kernel uses (CUDA cores, umulhi-based).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tb {
+
+// One NTT-friendly prime with everything the kernels need about it.
+// roots[i] = psi^bitrev(i) (forward, bit-reversed order), inv_roots in the
+// scrambled order of the Gentleman-Sande pass; each entry {operand, Shoup quotient}.
+struct Mod {
+    uint64_t value;
+    uint64_t ratio_lo, ratio_hi;   // floor(2^128 / value)
+    uint64_t inv_n, inv_n_quo;     // N^-1 mod value and its Shoup quotient
+    uint64_t sroot, sroot_quo;     // last inverse-NTT root times N^-1, and its quotient
+    const ulonglong2 *roots;
+    const ulonglong2 *inv_roots;
+};
+
+__device__ __forceinline__ uint64_t mulhi(uint64_t a, uint64_t b) { return __umul64hi(a, b); }
+
+// x * w mod q in [0, 2q) for any 64-bit x (Shoup; wq = floor(w 2^64 / q)).
+__device__ __forceinline__ uint64_t mul_shoup_lazy(uint64_t x, uint64_t w, uint64_t wq, uint64_t q) {
+    return w * x - mulhi(x, wq) * q;
+}
+
+__device__ __forceinline__ uint64_t mul_shoup(uint64_t x, uint64_t w, uint64_t wq, uint64_t q) {
+    uint64_t r = mul_shoup_lazy(x, w, wq, q);
+    return r >= q ? r - q : r;
+}
+
+__device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t q) { return x >= q ? x - q : x; }
+
+__device__ __forceinline__ uint64_t add_mod(uint64_t a, uint64_t b, uint64_t q) { return csub(a + b, q); }
+
+__device__ __forceinline__ uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t q) {
+    return a >= b ? a - b : a + q - b;
+}
+
+__device__ __forceinline__ uint64_t neg_mod(uint64_t a, uint64_t q) { return a ? q - a : 0; }
+
+// x mod q for any 64-bit x: the quotient estimate floor(x * floor(2^128/q) / 2^128)
+// using only the high ratio word is off by at most one.
+__device__ __forceinline__ uint64_t reduce64(uint64_t x, const Mod &m) {
+    uint64_t qt = mulhi(x, m.ratio_hi);
+    return csub(x - qt * m.value, m.value);
+}
+
+// (hi:lo) mod q for a 128-bit value: Barrett reduction with the 128-bit ratio;
+// the truncated quotient is at most one below the true one.
+__device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo, const Mod &m) {
+    uint64_t c = mulhi(lo, m.ratio_lo);
+    uint64_t a_lo = lo * m.ratio_hi, a_hi = mulhi(lo, m.ratio_hi);
+    uint64_t t1 = a_lo + c;
+    uint64_t t3 = a_hi + (t1 < c);
+    uint64_t b_lo = hi * m.ratio_lo, b_hi = mulhi(hi, m.ratio_lo);
+    uint64_t t2 = t1 + b_lo;
+    uint64_t carry = b_hi + (t2 < t1);
+    uint64_t qt = hi * m.ratio_hi + t3 + carry;
+    return csub(lo - qt * m.value, m.value);
+}
+
+__device__ __forceinline__ uint64_t mul_mod(uint64_t a, uint64_t b, const Mod &m) {
+    return reduce128(mulhi(a, b), a * b, m);
+}
+
+// 128-bit accumulator helpers for lazy inner products.
+struct U128 {
+    uint64_t lo, hi;
+};
+
+__device__ __forceinline__ void mac128(U128 &acc, uint64_t a, uint64_t b) {
+    uint64_t lo = a * b, hi = mulhi(a, b);
+    acc.lo += lo;
+    acc.hi += hi + (acc.lo < lo);
+}
+
+// Layout helper: 64-bit coefficient index -> shared-memory slot. XOR-swizzling the
+// low four index bits with the next four keeps every radix pass of the NTT and
+// the contiguous copies free of bank conflicts.
+__device__ __forceinline__ int swz(int e) { return e ^ ((e >> 4) & 15); }
+
+}  // namespace tb
+
+#define TB_CUDA_TRY(expr)                                 \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return tb::status_from(_e); \
+    } while (0)

@@ -1,0 +1,511 @@
+// Batched key switching (relinearize, rotations / Galois automorphisms).
+//
+// Restates Evaluator::switchKeyInplace (src/evaluator.cpp:2310-2653): RNS digit
+// decomposition with one digit per data limb and one special prime, per-digit
+// NTT into every key modulus, inner product with the key, then division by the
+// special prime with rounding ("mod-down") added into the ciphertext. A batch of
+// ciphertexts goes through five launches:
+//   1. (CKKS) inverse NTT of every target limb;
+//   2. mod-up: one fused forward-NTT CTA per (ciphertext, digit j, key modulus i)
+//      whose load reduces digit j mod q_i;
+//   3. inner product of the digits with both key components (lazy 128-bit sums);
+//   4. inverse NTT of the special-prime accumulators with the rounding offset;
+//   5. mod-down: one fused NTT (CKKS) or inverse NTT (BFV/BGV) CTA per output limb
+//      whose epilogue subtracts the special-prime part, scales by q_k^-1 and adds
+//      into the ciphertext.
+// All values are exact residues, so the result is word-identical to the reference.
+#include <algorithm>
+
+#include "context.hpp"
+#include "hostmath.hpp"
+#include "trace.cuh"
+
+namespace tb {
+
+unsigned grid_for(uint64_t work, int threads);
+
+namespace {
+
+__device__ __forceinline__ uint64_t full_fwd(uint64_t v, uint64_t q) {
+    v = v >= 2 * q ? v - 2 * q : v;
+    return v >= q ? v - q : v;
+}
+
+// [P][limbs] limbs at base + p*stride + l*N -> out + p*ostride + l*N.
+template <bool FWD>
+struct StridedNttOp {
+    const uint64_t *in;
+    uint64_t *out;
+    uint64_t istride, ostride;
+    const Mod *mods;
+    int first, limbs, lazy, logn;
+    struct Ctx {
+        NttLimb lm;
+        const uint64_t *in;
+        uint64_t *out;
+    };
+    __device__ Ctx ctx(int b) const {
+        const int p = b / limbs, l = b % limbs;
+        Ctx c;
+        c.lm = make_limb(mods[first + l], 0);
+        c.in = in + (size_t)p * istride + ((size_t)l << logn);
+        c.out = out + (size_t)p * ostride + ((size_t)l << logn);
+        return c;
+    }
+    __device__ uint64_t load(const Ctx &c, int e) const { return c.in[e]; }
+    __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(c.in + e);
+        a = v.x;
+        b = v.y;
+    }
+    __device__ uint64_t fix(const Ctx &c, uint64_t v) const {
+        if (lazy) return v;
+        return FWD ? full_fwd(v, c.lm.q) : (v >= c.lm.q ? v - c.lm.q : v);
+    }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = fix(c, v); }
+    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
+        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(fix(c, a), fix(c, b));
+    }
+};
+
+// Step 2: forward NTT of digit j (coefficient form) reduced into key modulus i.
+struct ModUpOp {
+    const uint64_t *src;      // CKKS: inverse-transformed targets [B][L][N]; else targets
+    uint64_t sstride;         // words between ciphertexts in src
+    uint64_t *digits;         // [B][L][L+1][N]
+    const Mod *mods;
+    const uint64_t *chain;    // device copy of chain values (for the reduce test)
+    int L, K, ckks, logn;
+    struct Ctx {
+        NttLimb lm;
+        const uint64_t *in;
+        uint64_t *out;
+        uint64_t ratio_hi;
+        int reduce;
+    };
+    __device__ Ctx ctx(int b) const {
+        const int P = ckks ? L * L : L * (L + 1);
+        const int cb = b / P, p = b % P;
+        int j, i;
+        if (ckks) {
+            j = p / L;
+            const int ii = p % L;
+            i = ii + (ii >= j);
+        } else {
+            j = p / (L + 1);
+            i = p % (L + 1);
+        }
+        const int mi = i == L ? K - 1 : i;
+        const Mod &m = mods[mi];
+        Ctx c;
+        c.lm = make_limb(m, 0);
+        c.ratio_hi = m.ratio_hi;
+        c.reduce = mods[j].value > m.value;
+        c.in = src + (size_t)cb * sstride + ((size_t)j << logn);
+        c.out = digits + ((((size_t)cb * L + j) * (L + 1) + i) << logn);
+        return c;
+    }
+    __device__ uint64_t load(const Ctx &c, int e) const {
+        const uint64_t x = c.in[e];
+        if (!c.reduce) return x;
+        const uint64_t q = c.lm.q;
+        const uint64_t r = x - mulhi(x, c.ratio_hi) * q;
+        return r >= q ? r - q : r;
+    }
+    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
+        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(full_fwd(a, c.lm.q), full_fwd(b, c.lm.q));
+    }
+};
+
+// Step 3: acc[b][c][i] = sum_j digit(b, j, i) * key[j][c][mi] mod q_mi, two coefficients per thread.
+__global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
+                                uint64_t tstride, const uint64_t *__restrict__ key, uint64_t *__restrict__ acc,
+                                const Mod *__restrict__ mods, int L, int K, int ckks, int logn) {
+    const uint32_t n = 1u << logn;
+    const uint32_t e = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (e >= n) return;
+    const int i = blockIdx.y;
+    const size_t cb = blockIdx.z;
+    const int mi = i == L ? K - 1 : i;
+    const Mod m = mods[mi];
+    U128 a00{0, 0}, a01{0, 0}, a10{0, 0}, a11{0, 0};
+    for (int j = 0; j < L; j++) {
+        const uint64_t *d = (ckks && i == j) ? target + cb * tstride + ((size_t)j << logn)
+                                             : digits + (((cb * L + j) * (L + 1) + i) << logn);
+        const ulonglong2 dv = *reinterpret_cast<const ulonglong2 *>(d + e);
+        const ulonglong2 k0 = __ldg(reinterpret_cast<const ulonglong2 *>(key + (((size_t)(2 * j) * K + mi) << logn) + e));
+        const ulonglong2 k1 =
+            __ldg(reinterpret_cast<const ulonglong2 *>(key + (((size_t)(2 * j + 1) * K + mi) << logn) + e));
+        mac128(a00, dv.x, k0.x);
+        mac128(a01, dv.y, k0.y);
+        mac128(a10, dv.x, k1.x);
+        mac128(a11, dv.y, k1.y);
+    }
+    uint64_t *o0 = acc + (((cb * 2 + 0) * (L + 1) + i) << logn) + e;
+    uint64_t *o1 = acc + (((cb * 2 + 1) * (L + 1) + i) << logn) + e;
+    *reinterpret_cast<ulonglong2 *>(o0) = make_ulonglong2(reduce128(a00.hi, a00.lo, m), reduce128(a01.hi, a01.lo, m));
+    *reinterpret_cast<ulonglong2 *>(o1) = make_ulonglong2(reduce128(a10.hi, a10.lo, m), reduce128(a11.hi, a11.lo, m));
+}
+
+// Step 4: inverse NTT of the special-prime accumulator; CKKS/BFV add (q_k - 1)/2 for
+// rounding (src/evaluator.cpp:2587-2596), BGV keeps the canonical residue.
+struct SpecialInttOp {
+    const uint64_t *acc;
+    uint64_t *last;
+    const Mod *mods;
+    int L, K, bgv, logn;
+    struct Ctx {
+        NttLimb lm;
+        const uint64_t *in;
+        uint64_t *out;
+    };
+    __device__ Ctx ctx(int b) const {
+        Ctx c;
+        c.lm = make_limb(mods[K - 1], 0);
+        c.in = acc + (((size_t)b * (L + 1) + L) << logn);
+        c.out = last + ((size_t)b << logn);
+        return c;
+    }
+    __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(c.in + e);
+        a = v.x;
+        b = v.y;
+    }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        if (bgv) {
+            c.out[e] = v >= q ? v - q : v;
+        } else {
+            uint64_t x = v + (q >> 1);
+            x = x >= 2 * q ? x - 2 * q : x;
+            c.out[e] = x >= q ? x - q : x;
+        }
+    }
+};
+
+struct ModDownBase {
+    const uint64_t *acc;      // [B][2][L+1][N]
+    const uint64_t *last;     // [B][2][N]
+    uint64_t *ct;             // c0 at ct + b*cstride, c1 at + L*N
+    uint64_t cstride;
+    const Mod *mods;
+    const DropC *drop;        // row for the special prime: drop[K*K + j]
+    int L, K, logn;
+    struct Ctx {
+        NttLimb lm;
+        const uint64_t *acc;
+        const uint64_t *last;
+        uint64_t *ct;
+        uint64_t ratio_hi;
+        DropC d;
+        int reduce;
+    };
+    __device__ Ctx make(int b) const {
+        const int j = b % L, bc = b / L;  // bc = cb*2 + c
+        const int cb = bc >> 1, cc = bc & 1;
+        const Mod &m = mods[j];
+        Ctx c;
+        c.lm = make_limb(m, 0);
+        c.ratio_hi = m.ratio_hi;
+        c.d = drop[(size_t)K * K + j];
+        c.reduce = mods[K - 1].value > m.value;
+        c.acc = acc + (((size_t)bc * (L + 1) + j) << logn);
+        c.last = last + ((size_t)bc << logn);
+        c.ct = ct + (size_t)cb * cstride + (((size_t)cc * L + j) << logn);
+        return c;
+    }
+    __device__ uint64_t last_mod(const Ctx &c, int e) const {
+        const uint64_t r = c.last[e];
+        if (!c.reduce) return r;
+        const uint64_t q = c.lm.q;
+        const uint64_t x = r - mulhi(r, c.ratio_hi) * q;
+        return x >= q ? x - q : x;
+    }
+};
+
+// Step 5, CKKS: NTT of (r mod q_j) + fix, epilogue ct += (acc + 4 q_j - ntt) * q_k^-1.
+struct ModDownCkksOp : ModDownBase {
+    __device__ Ctx ctx(int b) const { return make(b); }
+    __device__ uint64_t load(const Ctx &c, int e) const { return last_mod(c, e) + c.d.fix; }
+    __device__ uint64_t fin(const Ctx &c, int e, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        const uint64_t x = c.acc[e] + 4 * q - v;
+        return add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), c.ct[e], q);
+    }
+    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
+        const uint64_t x = fin(c, e, a), y = fin(c, e + 1, b);
+        *reinterpret_cast<ulonglong2 *>(c.ct + e) = make_ulonglong2(x, y);
+    }
+};
+
+// Step 5, BFV: inverse NTT of acc, epilogue ct += (intt + 2 q_j - ((r mod q_j) + fix)) * q_k^-1.
+struct ModDownBfvOp : ModDownBase {
+    __device__ Ctx ctx(int b) const { return make(b); }
+    __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(c.acc + e);
+        a = v.x;
+        b = v.y;
+    }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        const uint64_t t = last_mod(c, e) + c.d.fix;
+        const uint64_t x = v + 2 * q - t;
+        c.ct[e] = add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), c.ct[e], q);
+    }
+};
+
+// Step 5, BGV (src/evaluator.cpp:2528-2583): k = -(r mod t) q_k^-1 mod t,
+// ct += (intt + 2 q_j - (k q_k mod q_j + r mod q_j)) * q_k^-1.
+struct ModDownBgvOp : ModDownBase {
+    Mod tm;
+    uint64_t inv_qk_t;
+    __device__ Ctx ctx(int b) const { return make(b); }
+    __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(c.acc + e);
+        a = v.x;
+        b = v.y;
+    }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        const uint64_t r = c.last[e];
+        uint64_t k = neg_mod(reduce64(r, tm), tm.value);
+        if (inv_qk_t != 1) k = mul_mod(k, inv_qk_t, tm);
+        const uint64_t kq = k - mulhi(k, c.ratio_hi) * q;
+        const uint64_t delta = mul_shoup(kq >= q ? kq - q : kq, c.d.lastmod, c.d.lastmod_quo, q);
+        const uint64_t x = v + 2 * q - (delta + last_mod(c, e));
+        c.ct[e] = add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), c.ct[e], q);
+    }
+};
+
+}  // namespace
+
+// Per-context device scratch is taken from the stream-ordered pool of the device.
+struct Scratch {
+    void *p = nullptr;
+    cudaStream_t s;
+    explicit Scratch(cudaStream_t st) : s(st) {}
+    cudaError_t alloc(size_t bytes) { return cudaMallocAsync(&p, bytes, s); }
+    ~Scratch() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+void ensure_pool_retains(int device);
+
+// target[b] (L limbs) at target + b*tstride; ct[b] (2 polys, L limbs) at ct + b*cstride.
+int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct, uint64_t cstride,
+              const uint64_t *key, uint64_t B, cudaStream_t s) {
+    const int K = (int)c.chain.size();
+    if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
+    if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
+    if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
+    if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 16384");
+    if (!target || !ct || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (B == 0) return TB_OK;
+    const uint64_t n = c.n;
+    if (!tstride) tstride = (uint64_t)L * n;
+    if (!cstride) cstride = 2ull * L * n;
+    const bool ckks = c.scheme == SCHEME_CKKS;
+    const int pairs = ckks ? L * L : L * (L + 1);
+    const size_t per_ct = ((ckks ? (size_t)L : 0) + (size_t)L * (L + 1) + 2ull * (L + 1) + 2) * n * 8;
+    // chunk the batch so one chunk's intermediates stay in L2 (126 MB)
+    const size_t budget = 48ull << 20;
+    uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(B, budget / per_ct));
+    ensure_pool_retains(c.device);
+    Scratch scr(s);
+    cudaError_t e = scr.alloc(per_ct * chunk);
+    if (e != cudaSuccess) return status_from(e);
+    uint64_t *base = (uint64_t *)scr.p;
+    uint64_t *tgt = base;
+    uint64_t *digits = tgt + (ckks ? chunk * L * n : 0);
+    uint64_t *acc = digits + chunk * (uint64_t)L * (L + 1) * n;
+    uint64_t *last = acc + chunk * 2ull * (L + 1) * n;
+    const int logn = c.logn;
+    for (uint64_t b0 = 0; b0 < B; b0 += chunk) {
+        const uint64_t nb = std::min(chunk, B - b0);
+        const uint64_t *tg = target + b0 * tstride;
+        uint64_t *cc = ct + b0 * cstride;
+        if (ckks) {
+            StridedNttOp<false> op{tg, tgt, tstride, (uint64_t)L * n, c.d_mods, 0, L, 0, logn};
+            TraceScope ts("ks_target_intt", s);
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * L), logn, 1, s);
+            if (e != cudaSuccess) return status_from(e);
+        }
+        ModUpOp mu{ckks ? tgt : tg, ckks ? (uint64_t)L * n : tstride, digits, c.d_mods, nullptr, L, K, ckks, logn};
+        {
+            TraceScope ts("ks_modup_ntt", s);
+            e = dispatch_ntt<true>(logn, mu, (unsigned)(nb * pairs), 0, 0, s);
+        }
+        if (e != cudaSuccess) return status_from(e);
+        const int threads = 128;
+        dim3 grid((unsigned)((n / 2 + threads - 1) / threads), L + 1, (unsigned)nb);
+        {
+            TraceScope ts("ks_inner_product", s);
+            ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, key, acc, c.d_mods, L, K, ckks, logn);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return status_from(e);
+        SpecialInttOp si{acc, last, c.d_mods, L, K, c.scheme == SCHEME_BGV, logn};
+        {
+            TraceScope ts("ks_special_intt", s);
+            e = dispatch_ntt<false>(logn, si, (unsigned)(nb * 2), logn, 1, s);
+        }
+        if (e != cudaSuccess) return status_from(e);
+        ModDownBase mb{acc, last, cc, cstride, c.d_mods, c.d_drop, L, K, logn};
+        TraceScope ts("ks_moddown", s);
+        if (ckks) {
+            ModDownCkksOp op{mb};
+            e = dispatch_ntt<true>(logn, op, (unsigned)(nb * 2 * L), 0, 0, s);
+        } else if (c.scheme == SCHEME_BFV) {
+            ModDownBfvOp op{mb};
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * 2 * L), logn, 1, s);
+        } else {
+            ModDownBgvOp op{mb, c.t_mod, c.inv_qlast_t[K]};
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * 2 * L), logn, 1, s);
+        }
+        if (e != cudaSuccess) return status_from(e);
+    }
+    return TB_OK;
+}
+
+// ------------------------------------------------------------------ Galois
+
+namespace {
+
+// Coefficient-domain X -> X^elt with the negacyclic sign (GaloisTool::applyGalois,
+// src/utils/galois.cpp:143-165): c0 -> out c0, c1 -> target, out c1 cleared.
+__global__ void galois_coeff_kernel(const uint64_t *__restrict__ in, uint64_t istride, uint64_t *__restrict__ out0,
+                                    uint64_t ostride, uint64_t *__restrict__ tgt, uint64_t tstride,
+                                    uint64_t *__restrict__ out1, const Mod *__restrict__ mods, int L, int logn,
+                                    uint32_t elt) {
+    const uint32_t n = 1u << logn;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = blockIdx.y;
+    const size_t cb = blockIdx.z;
+    const uint64_t q = mods[j].value;
+    const uint64_t raw = (uint64_t)i * elt;
+    const uint32_t idx = (uint32_t)(raw & (n - 1));
+    const bool neg = (raw >> logn) & 1;
+    const uint64_t *src = in + cb * istride + ((size_t)j << logn);
+    uint64_t v0 = src[i], v1 = src[((size_t)L << logn) + i];
+    if (neg) {
+        v0 = neg_mod(v0, q);
+        v1 = neg_mod(v1, q);
+    }
+    out0[cb * ostride + ((size_t)j << logn) + idx] = v0;
+    tgt[cb * tstride + ((size_t)j << logn) + idx] = v1;
+    out1[cb * ostride + ((size_t)j << logn) + i] = 0;
+}
+
+// NTT-domain permutation (GaloisTool::applyGaloisNtt, src/utils/galois.cpp:167-177).
+__global__ void galois_ntt_kernel(const uint64_t *__restrict__ in, uint64_t istride, uint64_t *__restrict__ out0,
+                                  uint64_t ostride, uint64_t *__restrict__ tgt, uint64_t tstride,
+                                  uint64_t *__restrict__ out1, const uint32_t *__restrict__ perm, int L, int logn) {
+    const uint32_t n = 1u << logn;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = blockIdx.y;
+    const size_t cb = blockIdx.z;
+    const uint32_t p = __ldg(&perm[i]);
+    const uint64_t *src = in + cb * istride + ((size_t)j << logn);
+    out0[cb * ostride + ((size_t)j << logn) + i] = src[p];
+    tgt[cb * tstride + ((size_t)j << logn) + i] = src[((size_t)L << logn) + p];
+    out1[cb * ostride + ((size_t)j << logn) + i] = 0;
+}
+
+}  // namespace
+
+// Device permutation table of an element, built and uploaded on first use
+// (GaloisTool::generateTableNtt, src/utils/galois.cpp:18-43).
+int galois_ntt_table(Context &c, uint32_t elt, const uint32_t **out) {
+    std::lock_guard<std::mutex> g(c.galois_mu);
+    auto it = c.galois_ntt.find(elt);
+    if (it != c.galois_ntt.end()) {
+        *out = it->second;
+        return TB_OK;
+    }
+    const uint32_t n = c.n;
+    std::vector<uint32_t> t(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t rev = host::bitrev(n + i, c.logn + 1);
+        uint64_t raw = ((uint64_t)elt * rev) >> 1;
+        raw &= (uint64_t)(n - 1);
+        t[i] = host::bitrev((uint32_t)raw, c.logn);
+    }
+    uint32_t *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, n * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(d, t.data(), n * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (d) cudaFree(d);
+        return status_from(e);
+    }
+    c.galois_ntt[elt] = d;
+    *out = d;
+    return TB_OK;
+}
+
+// out[b] = apply_galois(in[b], elt) key-switched with the Galois key of elt
+// (Evaluator::applyGaloisInplace, src/evaluator.cpp:2153-2249).
+int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
+                 uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s) {
+    const uint32_t n = c.n;
+    if (!(elt & 1) || elt >= 2 * n) return set_error(TB_ERR_INVALID_ARGUMENT, "Galois element is not valid");
+    if (L < 1 || L > (int)c.chain.size() - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
+    if (!in || !out || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (B == 0) return TB_OK;
+    if (!istride) istride = 2ull * L * n;
+    if (!ostride) ostride = 2ull * L * n;
+    const bool inplace = in == out || (out < in + B * istride && in < out + B * ostride);
+    ensure_pool_retains(c.device);
+    Scratch scr(s);
+    const uint64_t tstride = (uint64_t)L * n;
+    const uint64_t ostride_w = inplace ? 2ull * L * n : ostride;
+    cudaError_t e = scr.alloc(B * tstride * 8 + (inplace ? B * 2ull * L * n * 8 : 0));
+    if (e != cudaSuccess) return status_from(e);
+    uint64_t *tgt = (uint64_t *)scr.p;
+    uint64_t *dst = inplace ? tgt + B * tstride : out;
+    dim3 grid((n + 255) / 256, L, (unsigned)B);
+    {
+    TraceScope ts("galois_permute", s);
+    if (c.scheme == SCHEME_CKKS) {
+        const uint32_t *perm = nullptr;
+        int st = galois_ntt_table(c, elt, &perm);
+        if (st != TB_OK) return st;
+        galois_ntt_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n, perm, L,
+                                               c.logn);
+    } else {
+        galois_coeff_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n,
+                                                 c.d_mods, L, c.logn, elt);
+    }
+    e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return status_from(e);
+    int st = keyswitch(c, L, tgt, tstride, dst, ostride_w, key, B, s);
+    if (st != TB_OK) return st;
+    if (inplace) {
+        e = cudaMemcpy2DAsync(out, ostride * 8, dst, ostride_w * 8, 2ull * L * n * 8, B, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return status_from(e);
+    }
+    return TB_OK;
+}
+
+// GaloisTool::getEltFromStep (src/utils/galois.cpp:45-88), generator 3.
+int galois_elt_from_step(const Context &c, int step, uint32_t *elt) {
+    const uint32_t n = c.n, m = 2 * n;
+    if (step == 0) {
+        *elt = m - 1;
+        return TB_OK;
+    }
+    const bool neg = step < 0;
+    uint32_t pos = (uint32_t)(neg ? -step : step);
+    if (pos >= (n >> 1)) return set_error(TB_ERR_INVALID_ARGUMENT, "step count too large");
+    pos &= m - 1;
+    uint32_t k = neg ? (n >> 1) - pos : pos;
+    uint64_t g = 1;
+    while (k--) g = (g * 3) & (m - 1);
+    *elt = (uint32_t)g;
+    return TB_OK;
+}
+
+}  // namespace tb

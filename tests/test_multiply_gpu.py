@@ -1,0 +1,83 @@
+"""Parity of batched ciphertext multiplication (BFV BEHZ, BGV, CKKS) with the oracle,
+bit-exact, through the C ABI."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import tb_capi  # noqa: E402
+
+BFV, CKKS, BGV = 1, 2, 3
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+def _rand(rng, moduli, n, lead):
+    shape = tuple(lead) + (len(moduli), n)
+    out = np.empty(shape, np.uint64)
+    for i, q in enumerate(moduli):
+        out[..., i, :] = rng.integers(0, q, tuple(lead) + (n,), dtype=np.uint64)
+    return out
+
+
+@pytest.mark.parametrize("n,bits,t", [
+    (4096, [36, 36, 37], 65537),
+    (8192, [43, 43, 44, 44, 44], None),
+    (16384, [48] * 9, None),
+    (64, [40, 40, 40, 40], None),
+])
+def test_bfv_multiply(orc, n, bits, t):
+    moduli = orc.coeff_modulus_create(n, bits)
+    if t is None:
+        t = orc.plain_modulus_batching(n, 20)
+    ctx = tb_capi.Context(BFV, n, moduli, t)
+    rng = np.random.default_rng(n)
+    K = len(moduli)
+    for L in sorted({K - 1, 1 if K > 2 else K - 1, K}):
+        data = moduli[:L]
+        B = 2
+        a = _rand(rng, data, n, (B, 2))
+        b = _rand(rng, data, n, (B, 2))
+        out = torch.empty((B, 3, L, n), dtype=torch.int64, device="cuda")
+        ctx("multiply", L, _dev(a), 0, _dev(b), 0, out, 0, B, None)
+        got = _host(out)
+        for i in range(B):
+            exp = orc.bfv_multiply(n, data, t, a[i], b[i])
+            assert np.array_equal(got[i], exp), (L, i)
+
+
+def test_bgv_and_ckks_multiply(orc):
+    n = 4096
+    logn = 12
+    moduli = orc.coeff_modulus_create(n, [40, 40, 41, 41])
+    t = orc.plain_modulus_batching(n, 20)
+    rng = np.random.default_rng(5)
+    L, B = 3, 2
+    data = moduli[:L]
+    a = _rand(rng, data, n, (B, 2))
+    b = _rand(rng, data, n, (B, 2))
+    for scheme in (BGV, CKKS):
+        ctx = tb_capi.Context(scheme, n, moduli, t if scheme == BGV else 0)
+        out = torch.empty((B, 3, L, n), dtype=torch.int64, device="cuda")
+        ctx("multiply", L, _dev(a), 0, _dev(b), 0, out, 0, B, None)
+        got = _host(out)
+        for i in range(B):
+            x, y = a[i], b[i]
+            if scheme == BGV:
+                x = orc.ntt_forward_rns(logn, data, x)
+                y = orc.ntt_forward_rns(logn, data, y)
+            d0 = orc.dyadic_rns(data, x[0], y[0])
+            d2 = orc.dyadic_rns(data, x[1], y[1])
+            s1 = orc.dyadic_rns(data, x[0], y[1]).astype(object) + orc.dyadic_rns(data, x[1], y[0]).astype(object)
+            d1 = np.stack([(s1[l] % data[l]).astype(np.uint64) for l in range(L)])
+            exp = np.stack([d0, d1, d2])
+            if scheme == BGV:
+                exp = orc.ntt_inverse_rns(logn, data, exp)
+            assert np.array_equal(got[i], exp), (scheme, i)

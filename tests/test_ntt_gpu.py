@@ -1,0 +1,96 @@
+"""Parity of the CUDA NTT / inverse NTT / dyadic product with the oracle, through the C ABI.
+
+Bit-exact for full and lazy outputs (the lazy ranges are reproduced exactly).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import tb_capi  # noqa: E402
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+@pytest.mark.parametrize("logn", list(range(1, 18)))
+def test_ntt_roundtrip_all_sizes(orc, logn):
+    n = 1 << logn
+    bits = [50, 50, 40] if logn >= 4 else [30, 30, 30]
+    moduli = orc.coeff_modulus_create(n, bits)
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(logn)
+    polys = 2 if logn < 15 else 1
+    x = np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(polys)])
+    d = _dev(x)
+    out = torch.empty_like(d)
+    for lazy in (0, 1):
+        ctx("ntt_forward", d, out, polys, 0, len(moduli), lazy, None)
+        got = _host(out)
+        exp = orc.ntt_forward_rns(logn, moduli, x, lazy=bool(lazy))
+        assert np.array_equal(got, exp), f"forward lazy={lazy}"
+        ctx("ntt_inverse", d, out, polys, 0, len(moduli), lazy, None)
+        got = _host(out)
+        exp = orc.ntt_inverse_rns(logn, moduli, x, lazy=bool(lazy))
+        assert np.array_equal(got, exp), f"inverse lazy={lazy}"
+    # in-place round trip returns the input
+    y = d.clone()
+    ctx("ntt_forward", y, y, polys, 0, len(moduli), 0, None)
+    ctx("ntt_inverse", y, y, polys, 0, len(moduli), 0, None)
+    assert torch.equal(y, d)
+
+
+def test_ntt_lazy_input_range(orc):
+    """Forward accepts [0, 4q) inputs and inverse [0, 2q) inputs, as the reference."""
+    logn, n = 12, 4096
+    moduli = orc.coeff_modulus_create(n, [60, 60])
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(3)
+    x = np.stack([rng.integers(0, 4 * q, n, dtype=np.uint64) for q in moduli])
+    d = _dev(x)
+    out = torch.empty_like(d)
+    ctx("ntt_forward", d, out, 1, 0, 2, 1, None)
+    assert np.array_equal(_host(out), orc.ntt_forward_rns(logn, moduli, x, lazy=True))
+    y = np.stack([rng.integers(0, 2 * q, n, dtype=np.uint64) for q in moduli])
+    d = _dev(y)
+    ctx("ntt_inverse", d, out, 1, 0, 2, 0, None)
+    assert np.array_equal(_host(out), orc.ntt_inverse_rns(logn, moduli, y))
+
+
+def test_dyadic_product(orc):
+    n = 8192
+    moduli = orc.coeff_modulus_create(n, [60, 50, 40, 36])
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(4)
+    a = np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(3)])
+    b = np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(3)])
+    out = torch.empty(a.shape, dtype=torch.int64, device="cuda")
+    ctx("dyadic_product", _dev(a), _dev(b), out, 3, 0, 4, None)
+    assert np.array_equal(_host(out), orc.dyadic_rns(moduli, a, b))
+
+
+def test_batched_ntt_sweep_shapes(orc):
+    """The raw NTT sweep: B polynomials x 8 limbs of 50-bit primes, forward, dyadic, inverse."""
+    for n, B in ((4096, 16), (16384, 4), (32768, 2)):
+        logn = n.bit_length() - 1
+        moduli = orc.coeff_modulus_create(n, [50] * 8)
+        ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+        rng = np.random.default_rng(n)
+        x = np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(B)])
+        y = np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(B)])
+        dx, dy = _dev(x), _dev(y)
+        ctx("ntt_forward", dx, dx, B, 0, 8, 0, None)
+        ctx("ntt_forward", dy, dy, B, 0, 8, 0, None)
+        dz = torch.empty_like(dx)
+        ctx("dyadic_product", dx, dy, dz, B, 0, 8, None)
+        ctx("ntt_inverse", dz, dz, B, 0, 8, 0, None)
+        ex = orc.ntt_forward_rns(logn, moduli, x)
+        ey = orc.ntt_forward_rns(logn, moduli, y)
+        ez = orc.ntt_inverse_rns(logn, moduli, orc.dyadic_rns(moduli, ex, ey))
+        assert np.array_equal(_host(dz), ez), n
