@@ -1,0 +1,436 @@
+"""Benchmark of the ciphertext-arithmetic hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (the batched CKKS evaluation the headline metric is quoted on):
+CKKS, N = 16384, coefficient modulus chain {60, 40 x 7, 60} bits (8 data limbs and
+one special prime), 64 ciphertext pairs per step. Each pair goes through
+multiply -> relinearize -> rescale_to_next -> rotate_vector(k), k = 2^(i mod 13)
+for pair i (13 Galois keys, k in {1, 2, 4, ..., 4096}). One op = one pair through
+that chain. Inputs and keys are seeded, uniformly random residues modulo each
+prime (the arithmetic performed is the same as on encrypted data).
+
+* ``value``: ops/s with inputs resident in HBM (CUDA events on the launch stream,
+  max over ranks). Inputs (2 x 128 MB) exceed the 126 MB L2 between steps.
+* ``e2e``: the same metric through the C ABI with host buffers: every step copies
+  both operand batches from pinned host memory and reads the results back.
+* ``roofline``: the dominant kernel from the library's per-launch event trace.
+* ``cpu_baseline``: the reference's own CPU implementation (compiled under
+  oracle/_ref) on a bounded sample of the same workload, one process per core.
+
+``--impl reference`` times only that CPU implementation as the benchmark line.
+With ``--gpus N`` (torchrun, one rank per GPU) every rank runs an independent
+replica of the workload; nothing is exchanged (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "seal-cuda_b200", "python"), os.path.join(ROOT, "oracle")]
+
+N = 16384
+BITS = [60] + [40] * 7 + [60]
+PAIRS = 64
+SCALE_BITS = 40
+STEPS_K = [1 << i for i in range(13)]
+METRIC = "HE mul+relin+rescale+rotate ops/s (CKKS N=16384, batched 64 pairs)"
+WORKLOAD = "ckks_n16384_L8_batch64_mul_relin_rescale_rotate"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------ clocks sampler
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ B200 arm
+def _rand_residues(torch, shape, moduli, gen):
+    """uint64 residues (stored as int64) uniform modulo moduli[l] along axis -2."""
+    out = torch.empty(shape, dtype=torch.int64, device="cuda")
+    for l, q in enumerate(moduli):
+        # q < 2^61: draw 62 random bits and reduce (negligible bias for a benchmark input)
+        x = torch.randint(0, 2 ** 62, shape[:-2] + (shape[-1],), dtype=torch.int64, device="cuda", generator=gen)
+        out[..., l, :] = torch.remainder(x, q)
+    return out
+
+
+def run_b200(args, rank, world):
+    import torch
+    import tb_capi
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    lib = tb_capi.lib()
+    arr = (ctypes.c_int * len(BITS))(*BITS)
+    mods = (ctypes.c_uint64 * len(BITS))()
+    tb_capi.check(lib.tb_coeff_modulus_create(ctypes.c_uint64(N), arr, len(BITS), mods))
+    moduli = [int(m) for m in mods]
+    ctx = tb_capi.Context(tb_capi.SCHEME_CKKS, N, moduli)
+    K = len(moduli)
+    L = K - 1
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    stream = torch.cuda.current_stream()
+
+    # keys: relinearization key and 13 Galois keys, key level [K-1][2][K][N]
+    rlk = _rand_residues(torch, (K - 1, 2, K, N), moduli, gen)
+    elts = []
+    for k in STEPS_K:
+        e = ctypes.c_uint32()
+        ctx("galois_elt_from_step", k, ctypes.byref(e))
+        elts.append(e.value)
+    gks = [_rand_residues(torch, (K - 1, 2, K, N), moduli, gen) for _ in STEPS_K]
+    # operands
+    A = _rand_residues(torch, (PAIRS, 2, L, N), moduli[:L], gen)
+    B = _rand_residues(torch, (PAIRS, 2, L, N), moduli[:L], gen)
+    T3 = torch.empty((PAIRS, 3, L, N), dtype=torch.int64, device="cuda")
+    R = torch.empty((PAIRS, 2, L - 1, N), dtype=torch.int64, device="cuda")
+    O = torch.empty((PAIRS, 2, L - 1, N), dtype=torch.int64, device="cuda")
+    # rotation groups: as many pairs per step k as pairs i with i mod 13 == g, laid out
+    # in contiguous runs so each Galois key serves one batched launch
+    runs, start = [], 0
+    for g in range(len(STEPS_K)):
+        cnt = sum(1 for i in range(PAIRS) if i % len(STEPS_K) == g)
+        runs.append((g, start, cnt))
+        start += cnt
+    words_r = 2 * (L - 1) * N
+
+    E = (ctypes.c_uint32 * len(runs))(*[elts[g] for g, _, _ in runs])
+    C = (ctypes.c_uint64 * len(runs))(*[cnt for _, _, cnt in runs])
+    P = (ctypes.c_void_p * len(runs))(*[gks[g].data_ptr() for g, _, _ in runs])
+
+    def step(a, b, out):
+        ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, stream)
+        ctx("relinearize", L, T3, 0, rlk, PAIRS, stream)
+        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, stream)
+        ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step(A, B, O)
+    barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    lib.tb_trace_enable(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(A, B, O)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    entries = (tb_capi_trace_entry * 64)()
+    cnt = ctypes.c_int()
+    tb_capi.check(lib.tb_trace_collect(entries, 64, ctypes.byref(cnt)))
+    lib.tb_trace_enable(0)
+    trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms)) for i in range(cnt.value)}
+    launches = sum(v[0] for v in trace.values()) // args.steps
+
+    # end to end through the C ABI with host buffers
+    hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
+    hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
+    hO = torch.empty(O.shape, dtype=torch.int64, pin_memory=True)
+    hA.copy_(A)
+    hB.copy_(B)
+    dA, dB = torch.empty_like(A), torch.empty_like(B)
+
+    def e2e_step():
+        dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        step(dA, dB, O)
+        hO.copy_(O, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    return {"ms": ms, "e2e_ms": e2e_ms, "trace": trace, "launches": launches, "clocks": clk,
+            "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
+
+
+class tb_capi_trace_entry(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
+
+
+def algorithmic_bytes_per_step(L):
+    """Bytes each traced kernel must move per step at this workload (8-byte words):
+    L data limbs at multiply/relinearize, L-1 after the rescale, K = L + 1 key limbs."""
+    n, B, W = N, PAIRS, 8
+    Lr = L - 1
+
+    def ks(l):  # per key switch of one ciphertext at level l (CKKS)
+        return {
+            "ks_target_intt": 2 * l * n * W,
+            "ks_modup_ntt": 2 * l * l * n * W,
+            "ks_inner_product": (l * l + l + 2 * (l + 1)) * n * W,   # digits + target in, accumulators out
+            "ks_special_intt": 2 * 2 * n * W,
+            "ks_moddown": 2 * l * 4 * n * W,                         # last, acc, ct in; ct out
+        }
+
+    out = {"tensor": B * 7 * L * n * W,
+           "rescale_last_intt": B * 2 * 2 * n * W,
+           "rescale_ntt": B * 2 * Lr * 3 * n * W,
+           "galois_permute": B * 5 * Lr * n * W}
+    for name, v in ks(L).items():
+        out[name] = B * v
+    for name, v in ks(Lr).items():
+        out[name] += B * v
+    # keys are read once per launch: relinearization key + one Galois key per group
+    out["ks_inner_product"] += 2 * L * (L + 1) * n * W + len(STEPS_K) * 2 * Lr * (Lr + 1) * n * W
+    return out
+
+
+def roofline(res, steps):
+    """Dominant kernel (most device time): algorithmic bytes per launch / mean launch time."""
+    trace = res["trace"]
+    alg = algorithmic_bytes_per_step(res["L"])
+    peak, kind = _peak_hbm()
+    table = {}
+    for name, (launches, total_ms) in trace.items():
+        per_launch_ms = total_ms / launches
+        b = alg.get(name)
+        gbs = (b * steps / launches) / (per_launch_ms * 1e-3) / 1e9 if b else None
+        table[name] = {"launches_per_step": launches // steps, "ms_per_step": round(total_ms / steps, 4),
+                       "GBps": round(gbs, 1) if gbs else None}
+    name = max(trace.items(), key=lambda kv: kv[1][1])[0]
+    launches, total_ms = trace[name]
+    per_launch_ms = total_ms / launches
+    bpl = alg[name] * steps / launches
+    achieved = bpl / (per_launch_ms * 1e-3) / 1e9
+    tr = TRAFFIC_PER_STEP.get(name)
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": round(tr * steps / launches) if tr else None,
+            "algorithmic_bytes_per_launch": round(bpl),
+            "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback",
+            "kernels": table}
+
+
+# DRAM bytes (read + write) per step of a kernel, from an ncu capture of a smaller
+# batch of this workload scaled by the units processed (see profiles/); absent until
+# captured.
+TRAFFIC_PER_STEP: dict = {}
+
+
+# -------------------------------------------------------------- CPU baseline
+def _ref_worker(args):
+    """One process: a reference session at the benchmark parameters, `ops` timed ops."""
+    ops, seed = args
+    import numpy as np
+    from oracle import RefSession
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libtroyref.so"))
+    moduli = _ref_moduli()
+    s = RefSession(2, N, moduli, 0, np.arange(seed, seed + 8, dtype=np.uint64))
+    rng = np.random.default_rng(seed)
+    v = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    w = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    a, b = s.encrypt_ckks(v, 2.0 ** SCALE_BITS), s.encrypt_ckks(w, 2.0 ** SCALE_BITS)
+    lib.ref_ct_free.argtypes = [C.c_void_p, C.c_int]
+    # warm: create the relinearization key and the Galois keys this worker uses
+    ks = [STEPS_K[(seed + i) % len(STEPS_K)] for i in range(ops)]
+    m = s.multiply(a, b)
+    r = s.relinearize(m)
+    rs = s.rescale(r)
+    for k in set(ks):
+        lib.ref_ct_free(s.h, s.rotate_vector(rs, k))
+    t0 = time.perf_counter()
+    for k in ks:
+        m = s.multiply(a, b)
+        r = s.relinearize(m)
+        rs = s.rescale(r)
+        o = s.rotate_vector(rs, k)
+        for x in (m, r, rs, o):
+            lib.ref_ct_free(s.h, x)
+    return ops, time.perf_counter() - t0
+
+
+def _ref_moduli():
+    from oracle import Oracle
+    return Oracle("ref").coeff_modulus_create(N, BITS)
+
+
+def cpu_reference(ops_per_worker, workers):
+    """ops/s of the reference CPU path, one independent session per process."""
+    ctxm = mp.get_context("spawn")
+    with ctxm.Pool(workers) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(ops_per_worker, 17 + 97 * i) for i in range(workers)])
+        wall = time.perf_counter() - t0
+    ops = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return ops / busy, ops, busy, wall
+
+
+def _cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker in the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    cores = _cpu_count()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        workers = cores
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, ops, busy, wall = cpu_reference(args.cpu_ops, workers)
+            if i >= args.warmup:
+                vals.append((v, ops, busy))
+        value = sum(v[1] for v in vals) / sum(v[2] for v in vals)
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "ops/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1e3 * statistics.mean(v[2] for v in vals), 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact modular)", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "global_batch": args.cpu_ops * workers, "seq_len": N,
+                           "parallelism": f"{workers} CPU processes"},
+                "cpu_baseline": {"value": round(value, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
+                                 "sample": f"{args.cpu_ops} ops per process x {workers} processes per step"},
+                "e2e": {"value": round(value, 3), "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_b200(args, rank, world)
+    ops_total = PAIRS * world
+    value = ops_total / (res["ms"] * 1e-3)
+    e2e = ops_total / (res["e2e_ms"] * 1e-3)
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libtroyref.so")):
+            workers = min(cores, 32)
+            v, ops, busy, wall = cpu_reference(args.cpu_ops, workers)
+            cpu = {"value": round(v, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
+                   "sample": f"{ops} ops ({args.cpu_ops} per process x {workers} processes), {busy:.1f} s"}
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "ops/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(res["ms"], 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact modular)",
+                "data": "synthetic: seeded uniform residues for ciphertexts and keys",
+                "config": {"workload": WORKLOAD, "global_batch": ops_total, "seq_len": N,
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "l2": "inputs (256 MB) larger than L2"},
+                "e2e": {"value": round(e2e, 2), "unit": "ops/s", "h2d_bytes_per_step": res["h2d"],
+                        "d2h_bytes_per_step": res["d2h"]},
+                "gpu_launches": res["launches"],
+                "roofline": roofline(res, args.steps),
+                "cpu_baseline": cpu,
+                "clocks": res["clocks"],
+                "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(res["trace"].items())}}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -53,6 +53,16 @@ int tb_context_create(int scheme, uint64_t poly_degree, const uint64_t *coeff_mo
                       uint64_t plain_modulus, tb_context **out);
 int tb_context_destroy(tb_context *ctx);
 
+/*
+ * NTT-friendly primes for a chain: for each requested bit size, the largest primes
+ * = 1 mod 2n below 2^bits, assigned from the smallest of each size's list first, as
+ * CoeffModulus::Create does (src/modulus.cpp:80-118). Host only.
+ */
+int tb_coeff_modulus_create(uint64_t poly_degree, const int *bit_sizes, int count, uint64_t *out);
+
+/* The batching plain modulus PlainModulus::Batching(n, bits) (src/modulus.h:528). Host only. */
+int tb_plain_modulus_batching(uint64_t poly_degree, int bits, uint64_t *out);
+
 /* Moduli with NTT tables, in table order: chain, then t (if batching), then Bsk primes. */
 int tb_context_moduli(const tb_context *ctx, uint64_t *out, int capacity, int *count);
 
@@ -141,6 +151,18 @@ int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, con
  */
 int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t *in, uint64_t in_stride,
                     uint64_t *out, uint64_t out_stride, const uint64_t *key, uint64_t batch, void *stream);
+
+/*
+ * Batched rotations with many keys in one pass: `groups` groups of ciphertexts laid
+ * out one after another in `in` / `out` (group g has counts[g] ciphertexts), group g
+ * rotated by galois_elt elts[g] and key-switched with keys[g] (a host array of device
+ * pointers to Galois keys). One launch sequence serves all groups, so a batch that
+ * mixes rotation steps fills the GPU like a single-key batch. No counterpart call in
+ * the reference (it rotates one ciphertext per call, src/evaluator_cuda.cu:2106-2163).
+ */
+int tb_apply_galois_groups(tb_context *ctx, int L, int groups, const uint32_t *elts, const uint64_t *counts,
+                           const uint64_t *in, uint64_t in_stride, uint64_t *out, uint64_t out_stride,
+                           const uint64_t *const *keys, void *stream);
 
 /* Galois element of a rotation step (0 = column swap). Replaces GaloisTool::getEltFromStep
    (src/utils/galois.cpp:45-88). */

@@ -21,6 +21,7 @@
 #include "utils/rlwe.h"
 
 #include <complex>
+#include <map>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -43,8 +44,16 @@ struct Session {
     std::unique_ptr<BatchEncoder> batch;
     std::unique_ptr<CKKSEncoder> ckks;
     std::vector<Ciphertext> cts;
+    std::map<uint32_t, GaloisKeys> gks;   // generated once per element
     SchemeType scheme;
 };
+
+const GaloisKeys &galois_keys_for(Session *s, uint32_t elt) {
+    auto it = s->gks.find(elt);
+    if (it == s->gks.end())
+        it = s->gks.emplace(elt, s->keygen->createGaloisKeys(std::vector<uint32_t>{elt})).first;
+    return it->second;
+}
 
 int add_ct(Session *s, Ciphertext &&c) {
     s->cts.push_back(std::move(c));
@@ -302,8 +311,13 @@ size_t ref_relin_key(void *h, uint64_t *out) {
 
 size_t ref_galois_key(void *h, uint32_t elt, uint64_t *out) {
     auto *s = static_cast<Session *>(h);
-    GaloisKeys gk = s->keygen->createGaloisKeys(std::vector<uint32_t>{elt});
-    return dump_kswitch(gk, GaloisKeys::getIndex(elt), out);
+    return dump_kswitch(galois_keys_for(s, elt), GaloisKeys::getIndex(elt), out);
+}
+
+// Drops a stored ciphertext's data (keeps ids stable) so long timing loops stay bounded.
+void ref_ct_free(void *h, int id) {
+    auto *s = static_cast<Session *>(h);
+    if (id >= 0 && id < (int)s->cts.size()) s->cts[id] = Ciphertext();
 }
 
 int ref_ct_encrypt_slots(void *h, const uint64_t *slots, size_t count) {
@@ -403,7 +417,7 @@ int ref_ct_rotate(void *h, int a, int kind, int step) {
     try {
         auto tool = s->context->keyContextData()->galoisTool();
         uint32_t elt = kind == 1 ? tool->getEltFromStep(0) : tool->getEltFromStep(step);
-        GaloisKeys gk = s->keygen->createGaloisKeys(std::vector<uint32_t>{elt});
+        const GaloisKeys &gk = galois_keys_for(s, elt);
         Ciphertext c;
         if (kind == 0) s->evaluator->rotateRows(s->cts.at(a), step, gk, c);
         else if (kind == 1) s->evaluator->rotateColumns(s->cts.at(a), gk, c);

@@ -6,6 +6,7 @@
 
 #include "../../include/troy_b200.h"
 #include "context.hpp"
+#include "hostmath.hpp"
 
 namespace tb {
 extern thread_local std::string g_last_error;
@@ -20,6 +21,9 @@ int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride,
 int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
                  uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s);
 int galois_elt_from_step(const Context &c, int step, uint32_t *elt);
+int apply_galois_groups(Context &c, int L, int groups, const uint32_t *elts, const uint64_t *counts,
+                        const uint64_t *in, uint64_t istride, uint64_t *out, uint64_t ostride,
+                        const uint64_t *const *keys, cudaStream_t s);
 void trace_enable(bool on);
 int trace_collect(std::map<std::string, std::pair<uint64_t, double>> &out);
 int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, uint64_t *out, uint64_t cstride_out,
@@ -67,6 +71,32 @@ int tb_context_destroy(tb_context *ctx) {
     delete ctx->c;
     delete ctx;
     return TB_OK;
+}
+
+int tb_coeff_modulus_create(uint64_t poly_degree, const int *bit_sizes, int count, uint64_t *out) {
+    using namespace tb::host;
+    if (!bit_sizes || !out || count < 1 || count > 64) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "bad bit sizes");
+    if (poly_degree < 2 || poly_degree > 131072 || (poly_degree & (poly_degree - 1)))
+        return set_error(tb::TB_ERR_INVALID_ARGUMENT, "poly degree must be a power of two in [2, 131072]");
+    std::map<int, int> need;
+    for (int i = 0; i < count; i++) {
+        if (bit_sizes[i] < 2 || bit_sizes[i] > 60) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "bit sizes must be in [2, 60]");
+        need[bit_sizes[i]]++;
+    }
+    std::map<int, std::vector<uint64_t>> lists;
+    for (auto &kv : need)
+        if (!get_primes(2 * poly_degree, kv.first, (size_t)kv.second, lists[kv.first]))
+            return set_error(tb::TB_ERR_INVALID_ARGUMENT, "failed to find enough qualifying primes");
+    for (int i = 0; i < count; i++) {
+        auto &l = lists[bit_sizes[i]];
+        out[i] = l.back();
+        l.pop_back();
+    }
+    return TB_OK;
+}
+
+int tb_plain_modulus_batching(uint64_t poly_degree, int bits, uint64_t *out) {
+    return tb_coeff_modulus_create(poly_degree, &bits, 1, out);
 }
 
 int tb_context_moduli(const tb_context *ctx, uint64_t *out, int capacity, int *count) {
@@ -126,6 +156,14 @@ int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t 
                     uint64_t *out, uint64_t out_stride, const uint64_t *key, uint64_t batch, void *stream) {
     return on_device(ctx, [&](tb::Context &c) {
         return tb::apply_galois(c, L, galois_elt, in, in_stride, out, out_stride, key, batch, S(stream));
+    });
+}
+
+int tb_apply_galois_groups(tb_context *ctx, int L, int groups, const uint32_t *elts, const uint64_t *counts,
+                           const uint64_t *in, uint64_t in_stride, uint64_t *out, uint64_t out_stride,
+                           const uint64_t *const *keys, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::apply_galois_groups(c, L, groups, elts, counts, in, in_stride, out, out_stride, keys, S(stream));
     });
 }
 

@@ -15,6 +15,7 @@
 //      into the ciphertext.
 // All values are exact residues, so the result is word-identical to the reference.
 #include <algorithm>
+#include <cstdlib>
 
 #include "context.hpp"
 #include "hostmath.hpp"
@@ -23,6 +24,34 @@
 namespace tb {
 
 unsigned grid_for(uint64_t work, int threads);
+
+// Up to MAX_GROUPS key-switching keys in one batched launch: ciphertexts
+// [first[g], first[g+1]) of the launch use key[g]. Passed by value as a kernel
+// parameter, so no device-side descriptor upload is needed.
+constexpr int MAX_GROUPS = 32;
+struct KeyGroups {
+    int count = 0;
+    const uint64_t *key[MAX_GROUPS];
+    uint32_t first[MAX_GROUPS + 1];
+    __device__ __forceinline__ const uint64_t *of(uint32_t cb) const {
+        int g = 0;
+        while (g + 1 < count && cb >= first[g + 1]) g++;
+        return key[g];
+    }
+    // The groups restricted to ciphertexts [b0, b0 + nb), rebased to start at 0.
+    KeyGroups slice(uint32_t b0, uint32_t nb) const {
+        KeyGroups r;
+        for (int g = 0; g < count; g++) {
+            const uint32_t lo = std::max(first[g], b0), hi = std::min(first[g + 1], b0 + nb);
+            if (lo >= hi) continue;
+            r.key[r.count] = key[g];
+            r.first[r.count] = lo - b0;
+            r.count++;
+        }
+        r.first[r.count] = nb;
+        return r;
+    }
+};
 
 namespace {
 
@@ -119,7 +148,7 @@ struct ModUpOp {
 
 // Step 3: acc[b][c][i] = sum_j digit(b, j, i) * key[j][c][mi] mod q_mi, two coefficients per thread.
 __global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
-                                uint64_t tstride, const uint64_t *__restrict__ key, uint64_t *__restrict__ acc,
+                                uint64_t tstride, KeyGroups keys, uint64_t *__restrict__ acc,
                                 const Mod *__restrict__ mods, int L, int K, int ckks, int logn) {
     const uint32_t n = 1u << logn;
     const uint32_t e = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
@@ -128,6 +157,7 @@ __global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint6
     const size_t cb = blockIdx.z;
     const int mi = i == L ? K - 1 : i;
     const Mod m = mods[mi];
+    const uint64_t *__restrict__ key = keys.of((uint32_t)cb);
     U128 a00{0, 0}, a01{0, 0}, a10{0, 0}, a11{0, 0};
     for (int j = 0; j < L; j++) {
         const uint64_t *d = (ckks && i == j) ? target + cb * tstride + ((size_t)j << logn)
@@ -293,14 +323,16 @@ struct Scratch {
 void ensure_pool_retains(int device);
 
 // target[b] (L limbs) at target + b*tstride; ct[b] (2 polys, L limbs) at ct + b*cstride.
-int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct, uint64_t cstride,
-              const uint64_t *key, uint64_t B, cudaStream_t s) {
+int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct,
+                     uint64_t cstride, const KeyGroups &keys, uint64_t B, cudaStream_t s) {
     const int K = (int)c.chain.size();
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
     if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
     if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
     if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 16384");
-    if (!target || !ct || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!target || !ct || keys.count < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    for (int g = 0; g < keys.count; g++)
+        if (!keys.key[g]) return set_error(TB_ERR_NO_KEY, "missing key-switching key");
     if (B == 0) return TB_OK;
     const uint64_t n = c.n;
     if (!tstride) tstride = (uint64_t)L * n;
@@ -308,8 +340,12 @@ int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride,
     const bool ckks = c.scheme == SCHEME_CKKS;
     const int pairs = ckks ? L * L : L * (L + 1);
     const size_t per_ct = ((ckks ? (size_t)L : 0) + (size_t)L * (L + 1) + 2ull * (L + 1) + 2) * n * 8;
-    // chunk the batch so one chunk's intermediates stay in L2 (126 MB)
-    const size_t budget = 48ull << 20;
+    // Whole batches per launch keep every stage's grid several waves deep; the batch is
+    // only split when its intermediates would exceed the scratch budget.
+    static const size_t budget = [] {
+        const char *v = getenv("TB_KS_SCRATCH_BYTES");
+        return v ? (size_t)strtoull(v, nullptr, 10) : (size_t)(2ull << 30);
+    }();
     uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(B, budget / per_ct));
     ensure_pool_retains(c.device);
     Scratch scr(s);
@@ -341,7 +377,8 @@ int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride,
         dim3 grid((unsigned)((n / 2 + threads - 1) / threads), L + 1, (unsigned)nb);
         {
             TraceScope ts("ks_inner_product", s);
-            ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, key, acc, c.d_mods, L, K, ckks, logn);
+            ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, keys.slice((uint32_t)b0, (uint32_t)nb),
+                                                     acc, c.d_mods, L, K, ckks, logn);
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return status_from(e);
@@ -368,21 +405,44 @@ int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride,
     return TB_OK;
 }
 
+int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct, uint64_t cstride,
+              const uint64_t *key, uint64_t B, cudaStream_t s) {
+    KeyGroups kg;
+    kg.count = 1;
+    kg.key[0] = key;
+    kg.first[0] = 0;
+    kg.first[1] = (uint32_t)B;
+    return keyswitch_groups(c, L, target, tstride, ct, cstride, kg, B, s);
+}
+
 // ------------------------------------------------------------------ Galois
 
 namespace {
 
 // Coefficient-domain X -> X^elt with the negacyclic sign (GaloisTool::applyGalois,
 // src/utils/galois.cpp:143-165): c0 -> out c0, c1 -> target, out c1 cleared.
+struct GaloisGroups {
+    int count = 0;
+    uint32_t elt[MAX_GROUPS];
+    const uint32_t *perm[MAX_GROUPS];
+    uint32_t first[MAX_GROUPS + 1];
+    __device__ __forceinline__ int of(uint32_t cb) const {
+        int g = 0;
+        while (g + 1 < count && cb >= first[g + 1]) g++;
+        return g;
+    }
+};
+
 __global__ void galois_coeff_kernel(const uint64_t *__restrict__ in, uint64_t istride, uint64_t *__restrict__ out0,
                                     uint64_t ostride, uint64_t *__restrict__ tgt, uint64_t tstride,
                                     uint64_t *__restrict__ out1, const Mod *__restrict__ mods, int L, int logn,
-                                    uint32_t elt) {
+                                    GaloisGroups gg) {
     const uint32_t n = 1u << logn;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int j = blockIdx.y;
     const size_t cb = blockIdx.z;
+    const uint32_t elt = gg.elt[gg.of((uint32_t)cb)];
     const uint64_t q = mods[j].value;
     const uint64_t raw = (uint64_t)i * elt;
     const uint32_t idx = (uint32_t)(raw & (n - 1));
@@ -401,12 +461,13 @@ __global__ void galois_coeff_kernel(const uint64_t *__restrict__ in, uint64_t is
 // NTT-domain permutation (GaloisTool::applyGaloisNtt, src/utils/galois.cpp:167-177).
 __global__ void galois_ntt_kernel(const uint64_t *__restrict__ in, uint64_t istride, uint64_t *__restrict__ out0,
                                   uint64_t ostride, uint64_t *__restrict__ tgt, uint64_t tstride,
-                                  uint64_t *__restrict__ out1, const uint32_t *__restrict__ perm, int L, int logn) {
+                                  uint64_t *__restrict__ out1, GaloisGroups gg, int L, int logn) {
     const uint32_t n = 1u << logn;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int j = blockIdx.y;
     const size_t cb = blockIdx.z;
+    const uint32_t *__restrict__ perm = gg.perm[gg.of((uint32_t)cb)];
     const uint32_t p = __ldg(&perm[i]);
     const uint64_t *src = in + cb * istride + ((size_t)j << logn);
     out0[cb * ostride + ((size_t)j << logn) + i] = src[p];
@@ -445,18 +506,57 @@ int galois_ntt_table(Context &c, uint32_t elt, const uint32_t **out) {
     return TB_OK;
 }
 
-// out[b] = apply_galois(in[b], elt) key-switched with the Galois key of elt
-// (Evaluator::applyGaloisInplace, src/evaluator.cpp:2153-2249).
-int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
-                 uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s) {
+// Groups of ciphertexts, group g rotated by elts[g] and key-switched with keys[g]
+// (Evaluator::applyGaloisInplace, src/evaluator.cpp:2153-2249, batched over many
+// elements): ciphertexts of group g follow those of group g-1 in `in` / `out`.
+int apply_galois_groups(Context &c, int L, int groups, const uint32_t *elts, const uint64_t *counts,
+                        const uint64_t *in, uint64_t istride, uint64_t *out, uint64_t ostride,
+                        const uint64_t *const *keys, cudaStream_t s) {
     const uint32_t n = c.n;
-    if (!(elt & 1) || elt >= 2 * n) return set_error(TB_ERR_INVALID_ARGUMENT, "Galois element is not valid");
     if (L < 1 || L > (int)c.chain.size() - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
-    if (!in || !out || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
-    if (B == 0) return TB_OK;
+    if (!in || !out || !elts || !counts || !keys || groups < 1)
+        return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     if (!istride) istride = 2ull * L * n;
     if (!ostride) ostride = 2ull * L * n;
-    const bool inplace = in == out || (out < in + B * istride && in < out + B * ostride);
+    uint64_t B = 0;
+    for (int g = 0; g < groups; g++) {
+        if (!(elts[g] & 1) || elts[g] >= 2 * n) return set_error(TB_ERR_INVALID_ARGUMENT, "Galois element is not valid");
+        if (!keys[g]) return set_error(TB_ERR_NO_KEY, "Galois key not present");
+        B += counts[g];
+    }
+    if (B == 0) return TB_OK;
+    if (groups > MAX_GROUPS) {
+        // split into launches of at most MAX_GROUPS groups
+        uint64_t done = 0;
+        for (int g0 = 0; g0 < groups; g0 += MAX_GROUPS) {
+            const int gc = std::min(MAX_GROUPS, groups - g0);
+            uint64_t cnt = 0;
+            for (int g = g0; g < g0 + gc; g++) cnt += counts[g];
+            int st = apply_galois_groups(c, L, gc, elts + g0, counts + g0, in + done * istride, istride,
+                                         out + done * ostride, ostride, keys + g0, s);
+            if (st != TB_OK) return st;
+            done += cnt;
+        }
+        return TB_OK;
+    }
+    if (B > 65535) return set_error(TB_ERR_INVALID_ARGUMENT, "at most 65535 ciphertexts per call");
+    GaloisGroups gg;
+    KeyGroups kg;
+    gg.count = kg.count = groups;
+    uint32_t f = 0;
+    for (int g = 0; g < groups; g++) {
+        gg.elt[g] = elts[g];
+        gg.perm[g] = nullptr;
+        if (c.scheme == SCHEME_CKKS) {
+            int st = galois_ntt_table(c, elts[g], &gg.perm[g]);
+            if (st != TB_OK) return st;
+        }
+        gg.first[g] = kg.first[g] = f;
+        kg.key[g] = keys[g];
+        f += (uint32_t)counts[g];
+    }
+    gg.first[groups] = kg.first[groups] = f;
+    const bool inplace = out < in + B * istride && in < out + B * ostride;
     ensure_pool_retains(c.device);
     Scratch scr(s);
     const uint64_t tstride = (uint64_t)L * n;
@@ -467,27 +567,29 @@ int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t i
     uint64_t *dst = inplace ? tgt + B * tstride : out;
     dim3 grid((n + 255) / 256, L, (unsigned)B);
     {
-    TraceScope ts("galois_permute", s);
-    if (c.scheme == SCHEME_CKKS) {
-        const uint32_t *perm = nullptr;
-        int st = galois_ntt_table(c, elt, &perm);
-        if (st != TB_OK) return st;
-        galois_ntt_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n, perm, L,
-                                               c.logn);
-    } else {
-        galois_coeff_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n,
-                                                 c.d_mods, L, c.logn, elt);
-    }
-    e = cudaGetLastError();
+        TraceScope ts("galois_permute", s);
+        if (c.scheme == SCHEME_CKKS)
+            galois_ntt_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n, gg,
+                                                   L, c.logn);
+        else
+            galois_coeff_kernel<<<grid, 256, 0, s>>>(in, istride, dst, ostride_w, tgt, tstride, dst + (size_t)L * n,
+                                                     c.d_mods, L, c.logn, gg);
+        e = cudaGetLastError();
     }
     if (e != cudaSuccess) return status_from(e);
-    int st = keyswitch(c, L, tgt, tstride, dst, ostride_w, key, B, s);
+    int st = keyswitch_groups(c, L, tgt, tstride, dst, ostride_w, kg, B, s);
     if (st != TB_OK) return st;
     if (inplace) {
         e = cudaMemcpy2DAsync(out, ostride * 8, dst, ostride_w * 8, 2ull * L * n * 8, B, cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return status_from(e);
     }
     return TB_OK;
+}
+
+int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
+                 uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s) {
+    const uint64_t *keys[1] = {key};
+    return apply_galois_groups(c, L, 1, &elt, &B, in, istride, out, ostride, keys, s);
 }
 
 // GaloisTool::getEltFromStep (src/utils/galois.cpp:45-88), generator 3.

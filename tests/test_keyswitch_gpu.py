@@ -166,3 +166,42 @@ def test_tensor_product(orc):
         x = orc.dyadic_rns(data, a[i, 0], b[i, 1]).astype(object) + orc.dyadic_rns(data, a[i, 1], b[i, 0]).astype(object)
         d1 = np.stack([(x[l] % data[l]).astype(np.uint64) for l in range(L)])
         assert np.array_equal(got[i, 0], d0) and np.array_equal(got[i, 1], d1) and np.array_equal(got[i, 2], d2)
+
+
+@pytest.mark.parametrize("scheme,n,bits,t", [PARAMS[0], PARAMS[2]])
+def test_apply_galois_groups(orc, scheme, n, bits, t):
+    """Several rotation steps with different keys in one batched call."""
+    import ctypes
+    moduli, t, ctx = _setup(orc, scheme, n, bits, t)
+    K = len(moduli)
+    logn = n.bit_length() - 1
+    rng = np.random.default_rng(19)
+    L = K - 1
+    data = moduli[:L]
+    steps = [1, 2, -5]
+    counts = [2, 1, 3]
+    B = sum(counts)
+    keys = [_rand(rng, moduli, n, (K - 1, 2)) for _ in steps]
+    dkeys = [_dev(k) for k in keys]
+    elts = [orc.galois_elt_from_step(logn, s_) for s_ in steps]
+    ct = _rand(rng, data, n, (B, 2))
+    din = _dev(ct)
+    dout = torch.empty_like(din)
+    E = (ctypes.c_uint32 * 3)(*elts)
+    C = (ctypes.c_uint64 * 3)(*counts)
+    P = (ctypes.c_void_p * 3)(*[k.data_ptr() for k in dkeys])
+    ctx("apply_galois_groups", L, 3, E, C, din, 0, dout, 0, P, None)
+    got = _host(dout)
+    b = 0
+    for g, cnt in enumerate(counts):
+        for _ in range(cnt):
+            if scheme == CKKS:
+                c0 = np.stack([orc.apply_galois_ntt(logn, elts[g], ct[b, 0, i]) for i in range(L)])
+                tg = np.stack([orc.apply_galois_ntt(logn, elts[g], ct[b, 1, i]) for i in range(L)])
+            else:
+                c0 = np.stack([orc.apply_galois(logn, elts[g], data[i], ct[b, 0, i]) for i in range(L)])
+                tg = np.stack([orc.apply_galois(logn, elts[g], data[i], ct[b, 1, i]) for i in range(L)])
+            exp = orc.keyswitch(scheme, logn, data + [moduli[-1]], t, tg, np.stack([c0, np.zeros_like(c0)]),
+                                _key_sub(keys[g], L))
+            assert np.array_equal(got[b], exp), (g, b)
+            b += 1
