@@ -41,7 +41,8 @@ sys.path[:0] = [os.path.join(ROOT, "seal-cuda_b200", "python"), os.path.join(ROO
 
 N = 16384
 BITS = [60] + [40] * 7 + [60]
-PAIRS = 64
+DEFAULT_PAIRS = 64
+PAIRS = DEFAULT_PAIRS
 SCALE_BITS = 40
 STEPS_K = [1 << i for i in range(13)]
 METRIC = "HE mul+relin+rescale+rotate ops/s (CKKS N=16384, batched 64 pairs)"
@@ -113,13 +114,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ B200 arm
 def _rand_residues(torch, shape, moduli, gen):
-    """uint64 residues (stored as int64) uniform modulo moduli[l] along axis -2."""
-    out = torch.empty(shape, dtype=torch.int64, device="cuda")
-    for l, q in enumerate(moduli):
-        # q < 2^61: draw 62 random bits and reduce (negligible bias for a benchmark input)
-        x = torch.randint(0, 2 ** 62, shape[:-2] + (shape[-1],), dtype=torch.int64, device="cuda", generator=gen)
-        out[..., l, :] = torch.remainder(x, q)
-    return out
+    """uint64 residues (stored as int64) uniform modulo moduli[l] along axis -2 (two launches)."""
+    # q < 2^61: 62 random bits reduced mod q (negligible bias for a benchmark input)
+    x = torch.randint(0, 2 ** 62, shape, dtype=torch.int64, device="cuda", generator=gen)
+    q = torch.tensor(moduli, dtype=torch.int64, device="cuda").view(len(moduli), 1)
+    return torch.remainder(x, q)
 
 
 def run_b200(args, rank, world):
@@ -186,10 +185,12 @@ def run_b200(args, rank, world):
     clocks.start()
     lib.tb_trace_enable(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     e0.record(stream)
     for _ in range(args.steps):
         step(A, B, O)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
@@ -246,7 +247,7 @@ def algorithmic_bytes_per_step(L):
     def ks(l):  # per key switch of one ciphertext at level l (CKKS)
         return {
             "ks_target_intt": 2 * l * n * W,
-            "ks_modup_ntt": 2 * l * l * n * W,
+            "ks_modup_ntt": (l + l * l) * n * W,                     # each target limb in once, L*L digits out
             "ks_inner_product": (l * l + l + 2 * (l + 1)) * n * W,   # digits + target in, accumulators out
             "ks_special_intt": 2 * 2 * n * W,
             "ks_moddown": 2 * l * 4 * n * W,                         # last, acc, ct in; ct out
@@ -358,6 +359,7 @@ def _cpu_count():
 
 # ---------------------------------------------------------------------- main
 def main():
+    global PAIRS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -365,7 +367,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker in the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
+                    help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
+    PAIRS = args.pairs
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     cores = _cpu_count()
