@@ -143,6 +143,23 @@ int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, con
                    void *stream);
 
 /*
+ * tb_relinearize for callers that cannot allocate device memory at call time (for
+ * example a serving loop that has budgeted all of HBM up front and must not stall on
+ * the allocator or fail a request with an out-of-memory error, or code running while
+ * another allocator owns the free memory). No counterpart in the reference: it is an
+ * addition of this library. Same arguments and result as tb_relinearize, but it
+ * calls no allocator: it works out of a 16 MiB scratch array in the library's device
+ * image (held on every GPU that loads the library until exit), one chunk of the
+ * batch at a time. A level whose single-ciphertext scratch exceeds 16 MiB is
+ * rejected with TB_ERR_INVALID_ARGUMENT (e.g. CKKS N=16384 fits up to L=8). The first
+ * call on a device looks up the array's device address; make that first call before
+ * any stream capture. All calls share the array: calls that overlap on the GPU race,
+ * so serialise them (one stream, one thread at a time).
+ */
+int tb_relinearize_noalloc(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key,
+                           uint64_t batch, void *stream);
+
+/*
  * Applies the Galois automorphism `galois_elt` to `batch` size-2 ciphertexts and
  * key-switches with that element's Galois key: coefficient-domain permutation for
  * BFV/BGV, NTT-domain permutation for CKKS. in may equal out. Replaces

@@ -21,6 +21,8 @@ int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride,
 int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,
                  uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s);
 int galois_elt_from_step(const Context &c, int step, uint32_t *elt);
+int relinearize_noalloc(const Context &c, int L, uint64_t *ct3, uint64_t cstride, const uint64_t *key, uint64_t B,
+                        cudaStream_t s);
 int apply_galois_groups(Context &c, int L, int groups, const uint32_t *elts, const uint64_t *counts,
                         const uint64_t *in, uint64_t istride, uint64_t *out, uint64_t ostride,
                         const uint64_t *const *keys, cudaStream_t s);
@@ -149,6 +151,13 @@ int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, con
         const uint64_t stride = ct_stride ? ct_stride : 3ull * L * c.n;
         if (!ct) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
         return tb::keyswitch(c, L, ct + 2ull * L * c.n, stride, ct, stride, key, batch, S(stream));
+    });
+}
+
+int tb_relinearize_noalloc(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key,
+                           uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::relinearize_noalloc(c, L, ct, ct_stride, key, batch, S(stream));
     });
 }
 

@@ -16,6 +16,8 @@
 // All values are exact residues, so the result is word-identical to the reference.
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
+#include <string>
 
 #include "context.hpp"
 #include "hostmath.hpp"
@@ -590,6 +592,113 @@ int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t i
                  uint64_t ostride, const uint64_t *key, uint64_t B, cudaStream_t s) {
     const uint64_t *keys[1] = {key};
     return apply_galois_groups(c, L, 1, &elt, &B, in, istride, out, ostride, keys, s);
+}
+
+// ------------------------------------------------- allocation-free relinearize
+//
+// Some callers cannot allocate device memory when they relinearize: a serving loop
+// that has budgeted every byte of HBM up front and must neither stall on the
+// allocator nor fail a request half-way with an out-of-memory error, or code that
+// runs while another allocator owns the device's free memory. For them
+// tb_relinearize_noalloc works out of a fixed scratch array that lives in the
+// library's device image: every GPU that loads the library holds these
+// TB_NOALLOC_SCRATCH_BYTES until the process exits. A batch is processed in as many
+// ciphertexts at a time as fit; a single ciphertext that needs more than the array
+// holds is rejected. Every call shares the one array, so calls that overlap on the
+// GPU (different streams, or different host threads) race on it and must be
+// serialised by the caller. No word of the scratch needs to start at zero: each word
+// a call reads was written earlier in that same call.
+
+constexpr size_t TB_NOALLOC_SCRATCH_BYTES = 16ull << 20;  // 16 MiB: one L=8, N=16384 CKKS ciphertext
+static __device__ __align__(256) uint64_t g_noalloc_scratch[TB_NOALLOC_SCRATCH_BYTES / 8];
+
+// Device address of g_noalloc_scratch on the current device. In host code the
+// array's name only stands in for the symbol, so its address is asked for once per
+// device, with that device current, and cached.
+static int noalloc_scratch(int device, uint64_t **out) {
+    static std::mutex mu;
+    static uint64_t *addr[64] = {nullptr};
+    if (device < 0 || device >= 64) return set_error(TB_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return status_from(e);
+        addr[device] = (uint64_t *)p;
+    }
+    *out = addr[device];
+    return TB_OK;
+}
+
+int relinearize_noalloc(const Context &c, int L, uint64_t *ct3, uint64_t cstride, const uint64_t *key, uint64_t B,
+                        cudaStream_t s) {
+    const int K = (int)c.chain.size();
+    if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
+    if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
+    if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
+    if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 16384");
+    if (!ct3 || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (B == 0) return TB_OK;
+    const uint64_t n = c.n;
+    if (!cstride) cstride = 3ull * L * n;
+    const bool ckks = c.scheme == SCHEME_CKKS;
+    const int pairs = ckks ? L * L : L * (L + 1);
+    const size_t per_ct = ((ckks ? (size_t)L : 0) + (size_t)L * (L + 1) + 2ull * (L + 1) + 2) * n * 8;
+    if (per_ct > TB_NOALLOC_SCRATCH_BYTES)
+        return set_error(TB_ERR_INVALID_ARGUMENT,
+                         "relinearize without allocation needs " + std::to_string(per_ct) +
+                             " bytes of scratch for one ciphertext at this level; the static scratch holds " +
+                             std::to_string(TB_NOALLOC_SCRATCH_BYTES) + " bytes");
+    uint64_t *base = nullptr;
+    int st = noalloc_scratch(c.device, &base);
+    if (st != TB_OK) return st;
+    const uint64_t chunk = std::min<uint64_t>(B, TB_NOALLOC_SCRATCH_BYTES / per_ct);
+    uint64_t *tgt = base;
+    uint64_t *digits = tgt + (ckks ? chunk * L * n : 0);
+    uint64_t *acc = digits + chunk * (uint64_t)L * (L + 1) * n;
+    uint64_t *last = acc + chunk * 2ull * (L + 1) * n;
+    KeyGroups keys;
+    keys.count = 1;
+    keys.key[0] = key;
+    keys.first[0] = 0;
+    const int logn = c.logn;
+    const uint64_t tstride = cstride;
+    cudaError_t e;
+    for (uint64_t b0 = 0; b0 < B; b0 += chunk) {
+        const uint64_t nb = std::min(chunk, B - b0);
+        keys.first[1] = (uint32_t)nb;
+        uint64_t *cc = ct3 + b0 * cstride;
+        const uint64_t *tg = cc + 2ull * L * n;   // the third polynomial is the target
+        if (ckks) {
+            StridedNttOp<false> op{tg, tgt, tstride, (uint64_t)L * n, c.d_mods, 0, L, 0, logn};
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * L), logn, 1, s);
+            if (e != cudaSuccess) return status_from(e);
+        }
+        ModUpOp mu{ckks ? tgt : tg, ckks ? (uint64_t)L * n : tstride, digits, c.d_mods, nullptr, L, K, ckks, logn};
+        e = dispatch_ntt<true>(logn, mu, (unsigned)(nb * pairs), 0, 0, s);
+        if (e != cudaSuccess) return status_from(e);
+        const int threads = 128;
+        dim3 grid((unsigned)((n / 2 + threads - 1) / threads), L + 1, (unsigned)nb);
+        ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, keys, acc, c.d_mods, L, K, ckks, logn);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return status_from(e);
+        SpecialInttOp si{acc, last, c.d_mods, L, K, c.scheme == SCHEME_BGV, logn};
+        e = dispatch_ntt<false>(logn, si, (unsigned)(nb * 2), logn, 1, s);
+        if (e != cudaSuccess) return status_from(e);
+        ModDownBase mb{acc, last, cc, cstride, c.d_mods, c.d_drop, L, K, logn};
+        if (ckks) {
+            ModDownCkksOp op{mb};
+            e = dispatch_ntt<true>(logn, op, (unsigned)(nb * 2 * L), 0, 0, s);
+        } else if (c.scheme == SCHEME_BFV) {
+            ModDownBfvOp op{mb};
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * 2 * L), logn, 1, s);
+        } else {
+            ModDownBgvOp op{mb, c.t_mod, c.inv_qlast_t[K]};
+            e = dispatch_ntt<false>(logn, op, (unsigned)(nb * 2 * L), logn, 1, s);
+        }
+        if (e != cudaSuccess) return status_from(e);
+    }
+    return TB_OK;
 }
 
 // GaloisTool::getEltFromStep (src/utils/galois.cpp:45-88), generator 3.
