@@ -199,6 +199,83 @@ int tb_galois_elt_from_step(const tb_context *ctx, int step, uint32_t *elt);
 int tb_rescale_to_next(tb_context *ctx, int L, const uint64_t *in, uint64_t in_stride, uint64_t *out,
                        uint64_t out_stride, int size, uint64_t batch, void *stream);
 
+/* ------------------------------------------------- keys, encryption, decryption
+ *
+ * PRNG: `seed8` (8 words) reproduces a Blake2xbPRNGFactory constructed with that
+ * seed: every PRNG the operation creates starts that seed's stream at 0, exactly as
+ * the reference (src/randomgen.h:412-427), so keys and ciphertexts are word-identical
+ * to the reference's. NULL draws fresh random seeds from the host. Secret key
+ * [K][N] and public key [2][K][N] are at the key level (NTT form).
+ */
+
+/* KeyGenerator::generateSk (src/keygenerator.cpp:47-74): ternary sample, NTT. */
+int tb_keygen_secret(tb_context *ctx, const uint64_t *seed8, uint64_t *sk, void *stream);
+/* KeyGenerator::generatePk (src/keygenerator.cpp:76-99): symmetric encryption of zero. */
+int tb_keygen_public(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint64_t *pk, void *stream);
+/* KeyGenerator::createRelinKeys (src/keygenerator.cpp:101-124): key for s^2, [K-1][2][K][N]. */
+int tb_keygen_relin(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint64_t *key, void *stream);
+/* KeyGenerator::createGaloisKeysInternal (src/keygenerator.cpp:126-170): key for one element. */
+int tb_keygen_galois(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint32_t galois_elt,
+                     uint64_t *key, void *stream);
+
+/*
+ * Asymmetric encryption of `batch` plaintexts at level L (Encryptor::encrypt,
+ * src/encryptor_cuda.cu:92-237): BFV/BGV plaintexts are plain_count words mod t each
+ * (coefficient form), CKKS plaintexts [L][n] in NTT form; plain_stride words between
+ * plaintexts. plain NULL encrypts zero. Output [batch][2][L][n] (ct_stride words apart).
+ */
+int tb_encrypt(tb_context *ctx, const uint64_t *seed8, const uint64_t *pk, int L, const uint64_t *plain,
+               uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride, uint64_t batch,
+               void *stream);
+/* Symmetric encryption with the secret key (Encryptor::encryptSymmetric, src/encryptor_cuda.cuh). */
+int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
+                         uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride,
+                         uint64_t batch, void *stream);
+/*
+ * Decrypts `batch` ciphertexts of `size` polynomials at level L (DecryptorCuda::decrypt,
+ * src/decryptor_cuda.cu:92-328): BFV scale-and-round / BGV exact conversion (times
+ * correction^-1) give n words mod t per plaintext; CKKS gives [L][n] in NTT form.
+ */
+int tb_decrypt(tb_context *ctx, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t ct_stride,
+               uint64_t *plain, uint64_t plain_stride, uint64_t correction, uint64_t batch, void *stream);
+
+/* ------------------------------------------------------------ batch encoder */
+
+/* BatchEncoderCuda::encode (src/batchencoder_cuda.cu:42-100): `count` <= n slot values
+   mod t per plaintext -> n coefficients. Needs an NTT-friendly plain modulus. */
+int tb_batch_encode(tb_context *ctx, const uint64_t *slots, uint64_t slot_stride, uint64_t count, uint64_t *plain,
+                    uint64_t batch, void *stream);
+/* BatchEncoderCuda::decode (src/batchencoder_cuda.cu:182-265): n coefficients -> n slots. */
+int tb_batch_decode(tb_context *ctx, const uint64_t *plain, uint64_t *slots, uint64_t slot_stride, uint64_t batch,
+                    void *stream);
+
+/* ------------------------------------------------------ plaintext arithmetic */
+
+/*
+ * Multiplies `batch` ciphertexts of `size` polynomials at level L by plaintexts
+ * (EvaluatorCuda::multiplyPlain, src/evaluator_cuda.cu:1744-1850): BFV/BGV plaintexts
+ * of plain_count words mod t (centred lift, NTT, dyadic, inverse NTT), CKKS plaintexts
+ * [L][n] in NTT form. plain_stride 0 = one plaintext for every ciphertext.
+ */
+int tb_multiply_plain(tb_context *ctx, int L, int size, const uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                      uint64_t plain_stride, uint64_t plain_count, uint64_t *out, uint64_t out_stride,
+                      uint64_t batch, void *stream);
+/* c0 += plaintext (BFV scaled by Delta, BGV reduced, CKKS NTT form) (EvaluatorCuda::addPlain /
+   subPlain via scalingvariant_cuda, src/utils/scalingvariant_cuda.cu:21-128). */
+int tb_add_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                 uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream);
+int tb_sub_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                 uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream);
+
+/* Element-wise ciphertext add / sub / negate over `size` polynomials at level L
+   (kernel_util::kAddPolyCoeffmod / kSubPolyCoeffmod / kNegatePolyCoeffmod, src/kernelutils.cuh). */
+int tb_add(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+           uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+int tb_sub(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+           uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, uint64_t *out,
+              uint64_t out_stride, uint64_t batch, void *stream);
+
 /* ---------------------------------------------------------------- tracing */
 
 /* Per-kernel device time of the library's launches (CUDA events on each launch's

@@ -27,6 +27,26 @@ int apply_galois_groups(Context &c, int L, int groups, const uint32_t *elts, con
                         const uint64_t *in, uint64_t istride, uint64_t *out, uint64_t ostride,
                         const uint64_t *const *keys, cudaStream_t s);
 void trace_enable(bool on);
+int keygen_secret(Context &c, const uint64_t *seed8, uint64_t *sk, cudaStream_t s);
+int keygen_public(Context &c, const uint64_t *seed8, const uint64_t *sk, uint64_t *pk, cudaStream_t s);
+int keygen_relin(Context &c, const uint64_t *seed8, const uint64_t *sk, uint64_t *out, cudaStream_t s);
+int keygen_galois(Context &c, const uint64_t *seed8, const uint64_t *sk, uint32_t elt, uint64_t *out, cudaStream_t s);
+int encrypt(Context &c, const uint64_t *seed8, const uint64_t *pk, int L, const uint64_t *plain, uint64_t pstride,
+            uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t count, cudaStream_t s);
+int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
+                      uint64_t pstride, uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t count,
+                      cudaStream_t s);
+int decrypt(Context &c, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t cstride, uint64_t *out,
+            uint64_t ostride, uint64_t correction, uint64_t B, cudaStream_t s);
+int batch_encode(Context &c, const uint64_t *slots, uint64_t sstride, uint32_t count, uint64_t *out, uint64_t B,
+                 cudaStream_t s);
+int batch_decode(Context &c, const uint64_t *plain, uint64_t *slots, uint64_t sstride, uint64_t B, cudaStream_t s);
+int multiply_plain(Context &c, int L, int size, const uint64_t *ct, uint64_t cstride, const uint64_t *plain,
+                   uint64_t pstride, uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int add_sub(const Context &c, int op, int L, int size, const uint64_t *a, uint64_t astride, const uint64_t *b,
+            uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int add_plain(Context &c, int L, int negate, uint64_t *ct, uint64_t cstride, const uint64_t *plain, uint64_t pstride,
+              uint32_t pcount, uint64_t B, cudaStream_t s);
 int trace_collect(std::map<std::string, std::pair<uint64_t, double>> &out);
 int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, uint64_t *out, uint64_t cstride_out,
                     int size, uint64_t B, cudaStream_t s);
@@ -185,6 +205,111 @@ int tb_rescale_to_next(tb_context *ctx, int L, const uint64_t *in, uint64_t in_s
                        uint64_t out_stride, int size, uint64_t batch, void *stream) {
     return on_device(ctx, [&](tb::Context &c) {
         return tb::rescale_to_next(c, L, in, in_stride, out, out_stride, size, batch, S(stream));
+    });
+}
+
+int tb_keygen_secret(tb_context *ctx, const uint64_t *seed8, uint64_t *sk, void *stream) {
+    if (!sk) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
+    return on_device(ctx, [&](tb::Context &c) { return tb::keygen_secret(c, seed8, sk, S(stream)); });
+}
+
+int tb_keygen_public(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint64_t *pk, void *stream) {
+    if (!sk || !pk) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
+    return on_device(ctx, [&](tb::Context &c) { return tb::keygen_public(c, seed8, sk, pk, S(stream)); });
+}
+
+int tb_keygen_relin(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint64_t *key, void *stream) {
+    if (!sk || !key) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
+    return on_device(ctx, [&](tb::Context &c) { return tb::keygen_relin(c, seed8, sk, key, S(stream)); });
+}
+
+int tb_keygen_galois(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, uint32_t galois_elt, uint64_t *key,
+                     void *stream) {
+    if (!sk || !key) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
+    return on_device(ctx, [&](tb::Context &c) { return tb::keygen_galois(c, seed8, sk, galois_elt, key, S(stream)); });
+}
+
+int tb_encrypt(tb_context *ctx, const uint64_t *seed8, const uint64_t *pk, int L, const uint64_t *plain,
+               uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride, uint64_t batch,
+               void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+        return tb::encrypt(c, seed8, pk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch, S(stream));
+    });
+}
+
+int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
+                         uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride,
+                         uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+        return tb::encrypt_symmetric(c, seed8, sk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch,
+                                     S(stream));
+    });
+}
+
+int tb_decrypt(tb_context *ctx, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t ct_stride,
+               uint64_t *plain, uint64_t plain_stride, uint64_t correction, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::decrypt(c, sk, L, size, ct, ct_stride, plain, plain_stride, correction, batch, S(stream));
+    });
+}
+
+int tb_batch_encode(tb_context *ctx, const uint64_t *slots, uint64_t slot_stride, uint64_t count, uint64_t *plain,
+                    uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "values_matrix size is too large");
+        return tb::batch_encode(c, slots, slot_stride, (uint32_t)count, plain, batch, S(stream));
+    });
+}
+
+int tb_batch_decode(tb_context *ctx, const uint64_t *plain, uint64_t *slots, uint64_t slot_stride, uint64_t batch,
+                    void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::batch_decode(c, plain, slots, slot_stride, batch, S(stream)); });
+}
+
+int tb_multiply_plain(tb_context *ctx, int L, int size, const uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                      uint64_t plain_stride, uint64_t plain_count, uint64_t *out, uint64_t out_stride,
+                      uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+        return tb::multiply_plain(c, L, size, ct, ct_stride, plain, plain_stride, (uint32_t)plain_count, out,
+                                  out_stride, batch, S(stream));
+    });
+}
+
+int tb_add_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                 uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::add_plain(c, L, 0, ct, ct_stride, plain, plain_stride, (uint32_t)plain_count, batch, S(stream));
+    });
+}
+
+int tb_sub_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
+                 uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::add_plain(c, L, 1, ct, ct_stride, plain, plain_stride, (uint32_t)plain_count, batch, S(stream));
+    });
+}
+
+int tb_add(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+           uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::add_sub(c, 0, L, size, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_sub(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
+           uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::add_sub(c, 1, L, size, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, uint64_t *out,
+              uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::add_sub(c, 2, L, size, a, a_stride, nullptr, 0, out, out_stride, batch, S(stream));
     });
 }
 

@@ -27,6 +27,7 @@ Context::~Context() {
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     for (auto &kv : galois_ntt) cudaFree(kv.second);
+    if (d_slot_map) cudaFree(d_slot_map);
     for (auto &lv : levels) {
         if (lv.d_consts) cudaFree(lv.d_consts);
         if (lv.d_bsk_mods) cudaFree(lv.d_bsk_mods);

@@ -101,6 +101,7 @@ struct Context {
     // Galois NTT-domain permutation tables, built on first use per element.
     std::mutex galois_mu;
     std::unordered_map<uint32_t, uint32_t *> galois_ntt;
+    uint32_t *d_slot_map = nullptr;   // batch-encoder slot -> coefficient map
     ~Context();
 };
 
