@@ -249,6 +249,20 @@ int tb_batch_encode(tb_context *ctx, const uint64_t *slots, uint64_t slot_stride
 int tb_batch_decode(tb_context *ctx, const uint64_t *plain, uint64_t *slots, uint64_t slot_stride, uint64_t batch,
                     void *stream);
 
+/* ------------------------------------------------------------ CKKS encoder */
+
+/*
+ * CKKSEncoderCuda::encode (src/ckks_cuda.cu:314-453): `count` <= n/2 complex values
+ * per plaintext (device doubles, re/im interleaved, value_stride complex numbers
+ * apart) -> plaintexts [batch][L][n] in NTT form at level L with the given scale.
+ */
+int tb_ckks_encode(tb_context *ctx, int L, const double *values, uint64_t value_stride, uint64_t count,
+                   double scale, uint64_t *plain, uint64_t batch, void *stream);
+/* CKKSEncoderCuda::decode (src/ckks_cuda.cu:900-971): plaintexts [batch][L][n] (NTT form)
+   -> n/2 complex values each (value_stride complex numbers apart). */
+int tb_ckks_decode(tb_context *ctx, int L, const uint64_t *plain, double scale, double *values,
+                   uint64_t value_stride, uint64_t batch, void *stream);
+
 /* ------------------------------------------------------ plaintext arithmetic */
 
 /*

@@ -43,6 +43,10 @@ int batch_encode(Context &c, const uint64_t *slots, uint64_t sstride, uint32_t c
 int batch_decode(Context &c, const uint64_t *plain, uint64_t *slots, uint64_t sstride, uint64_t B, cudaStream_t s);
 int multiply_plain(Context &c, int L, int size, const uint64_t *ct, uint64_t cstride, const uint64_t *plain,
                    uint64_t pstride, uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int ckks_encode(Context &c, int L, const double *values, uint64_t vstride, uint32_t count, double scale, uint64_t *out,
+                uint64_t B, cudaStream_t s);
+int ckks_decode(Context &c, int L, const uint64_t *plain, double scale, double *values, uint64_t ostride, uint64_t B,
+                cudaStream_t s);
 int add_sub(const Context &c, int op, int L, int size, const uint64_t *a, uint64_t astride, const uint64_t *b,
             uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
 int add_plain(Context &c, int L, int negate, uint64_t *ct, uint64_t cstride, const uint64_t *plain, uint64_t pstride,
@@ -266,6 +270,21 @@ int tb_batch_encode(tb_context *ctx, const uint64_t *slots, uint64_t slot_stride
 int tb_batch_decode(tb_context *ctx, const uint64_t *plain, uint64_t *slots, uint64_t slot_stride, uint64_t batch,
                     void *stream) {
     return on_device(ctx, [&](tb::Context &c) { return tb::batch_decode(c, plain, slots, slot_stride, batch, S(stream)); });
+}
+
+int tb_ckks_encode(tb_context *ctx, int L, const double *values, uint64_t value_stride, uint64_t count,
+                   double scale, uint64_t *plain, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (count > c.n / 2) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "values_size is too large");
+        return tb::ckks_encode(c, L, values, value_stride, (uint32_t)count, scale, plain, batch, S(stream));
+    });
+}
+
+int tb_ckks_decode(tb_context *ctx, int L, const uint64_t *plain, double scale, double *values,
+                   uint64_t value_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::ckks_decode(c, L, plain, scale, values, value_stride, batch, S(stream));
+    });
 }
 
 int tb_multiply_plain(tb_context *ctx, int L, int size, const uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,

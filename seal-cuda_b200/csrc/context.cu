@@ -28,6 +28,7 @@ Context::~Context() {
     cudaSetDevice(device);
     for (auto &kv : galois_ntt) cudaFree(kv.second);
     if (d_slot_map) cudaFree(d_slot_map);
+    if (d_fft_roots) cudaFree(d_fft_roots);
     for (auto &lv : levels) {
         if (lv.d_consts) cudaFree(lv.d_consts);
         if (lv.d_bsk_mods) cudaFree(lv.d_bsk_mods);

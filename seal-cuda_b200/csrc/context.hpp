@@ -102,6 +102,7 @@ struct Context {
     std::mutex galois_mu;
     std::unordered_map<uint32_t, uint32_t *> galois_ntt;
     uint32_t *d_slot_map = nullptr;   // batch-encoder slot -> coefficient map
+    void *d_fft_roots = nullptr;      // CKKS special-FFT roots: [N] forward, [N] inverse (double2)
     ~Context();
 };
 
