@@ -263,6 +263,21 @@ int tb_ckks_encode(tb_context *ctx, int L, const double *values, uint64_t value_
 int tb_ckks_decode(tb_context *ctx, int L, const uint64_t *plain, double scale, double *values,
                    uint64_t value_stride, uint64_t batch, void *stream);
 
+/* CKKSEncoderCuda::encodePolynomial (src/ckks_cuda.cu:455-565): `count` <= n real
+   coefficients per plaintext (coeff_stride doubles apart) times scale, rounded, reduced
+   and transformed -> [batch][L][n] NTT form. */
+int tb_ckks_encode_polynomial(tb_context *ctx, int L, const double *coeffs, uint64_t coeff_stride, uint64_t count,
+                              double scale, uint64_t *plain, uint64_t batch, void *stream);
+/* CKKSEncoderCuda::decodePolynomial (src/ckks_cuda.cu:983-1040): n real coefficients
+   (centred, divided by scale) per plaintext. */
+int tb_ckks_decode_polynomial(tb_context *ctx, int L, const uint64_t *plain, double scale, double *coeffs,
+                              uint64_t coeff_stride, uint64_t batch, void *stream);
+/* CKKSEncoder::encode(double value, scale) (src/ckks.cpp:279-400): round(value*scale) in
+   every slot, one plaintext [L][n] in NTT form. */
+int tb_ckks_encode_double(tb_context *ctx, int L, double value, double scale, uint64_t *plain, void *stream);
+/* CKKSEncoder::encode(int64_t value) (src/ckks.cpp:402-440): the integer in every slot, scale 1. */
+int tb_ckks_encode_int64(tb_context *ctx, int L, int64_t value, uint64_t *plain, void *stream);
+
 /* ------------------------------------------------------ plaintext arithmetic */
 
 /*
@@ -280,6 +295,20 @@ int tb_add_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const
                  uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream);
 int tb_sub_plain(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *plain,
                  uint64_t plain_stride, uint64_t plain_count, uint64_t batch, void *stream);
+
+/* Lifts `batch` BFV/BGV plaintexts (plain_count words mod t) to level L and transforms
+   them -> [batch][L][n] NTT form (EvaluatorCuda::transformToNttInplace(Plaintext),
+   src/evaluator_cuda.cu:1869-1935). */
+int tb_plain_to_ntt(tb_context *ctx, int L, const uint64_t *plain, uint64_t plain_stride, uint64_t plain_count,
+                    uint64_t *out, uint64_t batch, void *stream);
+/* out = a * scalar mod q_l over `size` polynomials at level L
+   (kernel_util::kMultiplyPolyScalarCoeffmod, src/kernelutils.cuh; BGV correction balancing). */
+int tb_multiply_scalar(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, uint64_t scalar,
+                       uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+/* out = plain * scalar mod t over `count` words per plaintext (BGV addPlain's correction
+   factor, src/evaluator_cuda.cu:1597-1604). */
+int tb_plain_multiply_scalar(tb_context *ctx, const uint64_t *plain, uint64_t plain_stride, uint64_t count,
+                             uint64_t scalar, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
 
 /* Element-wise ciphertext add / sub / negate over `size` polynomials at level L
    (kernel_util::kAddPolyCoeffmod / kSubPolyCoeffmod / kNegatePolyCoeffmod, src/kernelutils.cuh). */

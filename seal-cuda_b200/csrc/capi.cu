@@ -52,6 +52,19 @@ int add_sub(const Context &c, int op, int L, int size, const uint64_t *a, uint64
 int add_plain(Context &c, int L, int negate, uint64_t *ct, uint64_t cstride, const uint64_t *plain, uint64_t pstride,
               uint32_t pcount, uint64_t B, cudaStream_t s);
 int trace_collect(std::map<std::string, std::pair<uint64_t, double>> &out);
+int multiply_scalar(Context &c, int L, int size, const uint64_t *a, uint64_t astride, uint64_t scalar, uint64_t *out,
+                    uint64_t ostride, uint64_t B, cudaStream_t s);
+int plain_multiply_scalar(Context &c, const uint64_t *a, uint64_t astride, uint64_t count, uint64_t scalar,
+                          uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int plain_to_ntt(Context &c, int L, const uint64_t *plain, uint64_t pstride, uint32_t pcount, uint64_t *out,
+                 uint64_t B, cudaStream_t s);
+int ckks_encode_polynomial(Context &c, int L, const double *values, uint64_t vstride, uint32_t count, double scale,
+                           uint64_t *out, uint64_t B, cudaStream_t s);
+int ckks_decode_polynomial(Context &c, int L, const uint64_t *plain, double scale, double *values, uint64_t ostride,
+                           uint64_t B, cudaStream_t s);
+int ckks_encode_double(Context &c, int L, double value, double scale, uint64_t *out, cudaStream_t s);
+int ckks_encode_int64(Context &c, int L, int64_t value, uint64_t *out, cudaStream_t s);
+
 int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, uint64_t *out, uint64_t cstride_out,
                     int size, uint64_t B, cudaStream_t s);
 }  // namespace tb
@@ -284,6 +297,51 @@ int tb_ckks_decode(tb_context *ctx, int L, const uint64_t *plain, double scale, 
                    uint64_t value_stride, uint64_t batch, void *stream) {
     return on_device(ctx, [&](tb::Context &c) {
         return tb::ckks_decode(c, L, plain, scale, values, value_stride, batch, S(stream));
+    });
+}
+
+int tb_ckks_encode_polynomial(tb_context *ctx, int L, const double *coeffs, uint64_t coeff_stride, uint64_t count,
+                              double scale, uint64_t *plain, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "values_size is too large");
+        return tb::ckks_encode_polynomial(c, L, coeffs, coeff_stride, (uint32_t)count, scale, plain, batch, S(stream));
+    });
+}
+
+int tb_ckks_decode_polynomial(tb_context *ctx, int L, const uint64_t *plain, double scale, double *coeffs,
+                              uint64_t coeff_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::ckks_decode_polynomial(c, L, plain, scale, coeffs, coeff_stride, batch, S(stream));
+    });
+}
+
+int tb_ckks_encode_double(tb_context *ctx, int L, double value, double scale, uint64_t *plain, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::ckks_encode_double(c, L, value, scale, plain, S(stream)); });
+}
+
+int tb_ckks_encode_int64(tb_context *ctx, int L, int64_t value, uint64_t *plain, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::ckks_encode_int64(c, L, value, plain, S(stream)); });
+}
+
+int tb_plain_to_ntt(tb_context *ctx, int L, const uint64_t *plain, uint64_t plain_stride, uint64_t plain_count,
+                    uint64_t *out, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+        return tb::plain_to_ntt(c, L, plain, plain_stride, (uint32_t)plain_count, out, batch, S(stream));
+    });
+}
+
+int tb_multiply_scalar(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, uint64_t scalar,
+                       uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::multiply_scalar(c, L, size, a, a_stride, scalar, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_plain_multiply_scalar(tb_context *ctx, const uint64_t *plain, uint64_t plain_stride, uint64_t count,
+                             uint64_t scalar, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::plain_multiply_scalar(c, plain, plain_stride, count, scalar, out, out_stride, batch, S(stream));
     });
 }
 

@@ -220,6 +220,28 @@ __global__ void ckks_gather(const double2 *__restrict__ a, double2 *__restrict__
     }
 }
 
+// a[b][i] = (v[b][i] * scale, 0) for i < count, 0 elsewhere (coefficient encode).
+__global__ void ckks_load_real(const double *__restrict__ vals, uint64_t vstride, uint32_t count, double scale,
+                               double2 *__restrict__ out, int logn, uint64_t B) {
+    const uint32_t n = 1u << logn;
+    const uint64_t total = B << logn;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = w >> logn;
+        const uint32_t i = (uint32_t)(w & (n - 1));
+        out[w] = make_double2(i < count ? __dmul_rn(vals[b * vstride + i], scale) : 0.0, 0.0);
+    }
+}
+
+__global__ void ckks_store_real(const double2 *__restrict__ a, double *__restrict__ out, uint64_t ostride, int logn,
+                                uint64_t B) {
+    const uint32_t n = 1u << logn;
+    const uint64_t total = B << logn;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = w >> logn;
+        out[b * ostride + (w & (n - 1))] = a[w].x;
+    }
+}
+
 }  // namespace
 
 // Complex root tables of the special FFT (CKKSEncoder constructor, src/ckks.cpp:62-77).
@@ -272,6 +294,23 @@ static int total_bits(const Context &c, int L) {
     return host::bit_count(host::product(c.chain.data(), L));
 }
 
+// Rounds the real parts of buf [B][N] into plaintexts [B][L][N] and transforms them;
+// fails with "encoded values are too large" when a coefficient reaches the modulus.
+static int round_reduce_ntt(Context &c, int L, double2 *buf, uint64_t *out, uint64_t B, cudaStream_t s) {
+    int *err = nullptr;
+    cudaError_t e = cudaMallocAsync(&err, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e != cudaSuccess) return status_from(e);
+    ckks_round_reduce<<<grid_for(B * c.n, 256), 256, 0, s>>>(buf, out, c.d_mods, L, c.logn, B, err, total_bits(c, L));
+    int herr = 0;
+    e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(err, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return status_from(e);
+    if (herr) return set_error(TB_ERR_INVALID_ARGUMENT, "encoded values are too large");
+    return ntt_forward(c, out, out, B, 0, L, false, s);
+}
+
 // values [B][vstride] complex (count used) -> plaintexts [B][L][N], NTT form.
 int ckks_encode(Context &c, int L, const double *values, uint64_t vstride, uint32_t count, double scale, uint64_t *out,
                 uint64_t B, cudaStream_t s) {
@@ -291,10 +330,7 @@ int ckks_encode(Context &c, int L, const double *values, uint64_t vstride, uint3
     if (r != TB_OK) return r;
     ensure_pool_retains(c.device);
     double2 *buf = nullptr;
-    int *err = nullptr;
     cudaError_t e = cudaMallocAsync(&buf, B * n * sizeof(double2), s);
-    if (e == cudaSuccess) e = cudaMallocAsync(&err, sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
     if (e != cudaSuccess) return status_from(e);
     {
         TraceScope ts("ckks_encode", s);
@@ -302,37 +338,96 @@ int ckks_encode(Context &c, int L, const double *values, uint64_t vstride, uint3
                                                               c.logn, B);
         for (int st = 0; st < c.logn; st++)
             fft_inv_stage<<<grid_for(B * n / 2, 256), 256, 0, s>>>(buf, iroots, c.logn, st, scale / (double)n, B);
-        ckks_round_reduce<<<grid_for(B * n, 256), 256, 0, s>>>(buf, out, c.d_mods, L, c.logn, B, err,
-                                                              total_bits(c, L));
     }
-    int herr = 0;
-    e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    r = round_reduce_ntt(c, L, buf, out, B, s);
     cudaFreeAsync(buf, s);
-    cudaFreeAsync(err, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return status_from(e);
-    if (herr) return set_error(TB_ERR_INVALID_ARGUMENT, "encoded values are too large");
-    return ntt_forward(c, out, out, B, 0, L, false, s);
+    return r;
 }
 
-// plaintexts [B][L][N] (NTT form) -> slot values [B][ostride] complex (N/2 used).
-int ckks_decode(Context &c, int L, const uint64_t *plain, double scale, double *values, uint64_t ostride, uint64_t B,
-                cudaStream_t s) {
-    using namespace host;
+// Real coefficients [B][vstride] (count <= N used) times scale, rounded, reduced and
+// transformed: CKKSEncoderCuda::encodePolynomialInternal (src/ckks_cuda.cu:455-565).
+int ckks_encode_polynomial(Context &c, int L, const double *values, uint64_t vstride, uint32_t count, double scale,
+                           uint64_t *out, uint64_t B, cudaStream_t s) {
     if (c.scheme != SCHEME_CKKS) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
-    const uint32_t n = c.n;
-    if (L < 1 || L > (int)c.chain.size() || L + 1 > MAXW) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level");
-    if (!(scale > 0) || (int)std::log2(scale) >= total_bits(c, L))
-        return set_error(TB_ERR_INVALID_ARGUMENT, "scale out of bounds");
-    if (!plain || !values) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    if (count > c.n) return set_error(TB_ERR_INVALID_ARGUMENT, "values_size is too large");
+    if (!out || (count && !values)) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     if (!B) return TB_OK;
-    if (!ostride) ostride = n / 2;
-    const uint32_t *map = nullptr;
-    double2 *roots, *iroots;
-    int r = slot_map(c, &map);
-    if (r == TB_OK) r = ckks_tables(c, &roots, &iroots);
-    if (r != TB_OK) return r;
-    // CRT constants of this level
+    if (!vstride) vstride = count;
+    ensure_pool_retains(c.device);
+    double2 *buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, B * c.n * sizeof(double2), s);
+    if (e != cudaSuccess) return status_from(e);
+    {
+        TraceScope ts("ckks_encode", s);
+        ckks_load_real<<<grid_for(B * c.n, 256), 256, 0, s>>>(values, vstride, count, scale, buf, c.logn, B);
+    }
+    const int r = round_reduce_ntt(c, L, buf, out, B, s);
+    cudaFreeAsync(buf, s);
+    return r;
+}
+
+int fill_limbs(Context &c, int L, const uint64_t *vals, uint64_t *out, uint64_t B, cudaStream_t s);
+
+// |x| mod q for a non-negative integral double x, through its base-2^64 digits.
+static uint64_t double_mod(double x, uint64_t q) {
+    const double two64 = 18446744073709551616.0;
+    std::vector<uint64_t> words;
+    while (x >= 1) {
+        words.push_back((uint64_t)std::fmod(x, two64));
+        x /= two64;
+    }
+    unsigned __int128 r = 0;
+    for (size_t k = words.size(); k-- > 0;) r = ((r << 64) | words[k]) % q;
+    return (uint64_t)r;
+}
+
+// The constant round(value * scale) in every slot: every NTT coefficient of limb l
+// equals the constant mod q_l (CKKSEncoder::encodeInternal(double), src/ckks.cpp:279-400).
+int ckks_encode_double(Context &c, int L, double value, double scale, uint64_t *out, cudaStream_t s) {
+    if (c.scheme != SCHEME_CKKS) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    const int bits = total_bits(c, L);
+    if (!(scale > 0) || (int)std::log2(scale) >= bits) return set_error(TB_ERR_INVALID_ARGUMENT, "scale out of bounds");
+    value *= scale;
+    if (value != 0.0 && (int)std::log2(std::fabs(value)) + 2 >= bits)
+        return set_error(TB_ERR_INVALID_ARGUMENT, "encoded value is too large");
+    double cd = std::round(value);
+    const bool neg = std::signbit(cd);
+    cd = std::fabs(cd);
+    std::vector<uint64_t> vals(L);
+    for (int l = 0; l < L; l++) {
+        const uint64_t q = c.chain[l];
+        const uint64_t r = double_mod(cd, q);
+        vals[l] = (neg && r) ? q - r : r;
+    }
+    TraceScope ts("ckks_encode", s);
+    return fill_limbs(c, L, vals.data(), out, 1, s);
+}
+
+// The integer `value` in every slot, scale 1 (CKKSEncoder::encodeInternal(int64_t),
+// src/ckks.cpp:402-440): residue ((uint64)value + q) mod q for negative values.
+int ckks_encode_int64(Context &c, int L, int64_t value, uint64_t *out, cudaStream_t s) {
+    if (c.scheme != SCHEME_CKKS) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    const uint64_t mag = value < 0 ? 0 - (uint64_t)value : (uint64_t)value;
+    if (host::bit_count(mag) + 2 >= total_bits(c, L))
+        return set_error(TB_ERR_INVALID_ARGUMENT, "encoded value is too large");
+    std::vector<uint64_t> vals(L);
+    for (int l = 0; l < L; l++) {
+        const uint64_t q = c.chain[l];
+        const uint64_t fill = value < 0 ? (uint64_t)value + q : (uint64_t)value;
+        vals[l] = fill % q;
+    }
+    TraceScope ts("ckks_encode", s);
+    return fill_limbs(c, L, vals.data(), out, 1, s);
+}
+
+// Inverse NTT, CRT compose, centre and scale by 1/scale: buf [B][N] (real parts).
+static int compose_level(Context &c, int L, const uint64_t *plain, double scale, double2 *buf, uint64_t B,
+                         cudaStream_t s) {
+    using namespace host;
+    const uint32_t n = c.n;
     const uint64_t *q = c.chain.data();
     auto Q = product(q, L);
     Q.resize(L, 0);
@@ -362,28 +457,82 @@ int ckks_decode(Context &c, int L, const uint64_t *plain, double scale, double *
     }
     ensure_pool_retains(c.device);
     uint64_t *tmp = nullptr, *dc = nullptr;
-    double2 *buf = nullptr;
     cudaError_t e = cudaMallocAsync(&tmp, 8ull * B * L * n, s);
-    if (e == cudaSuccess) e = cudaMallocAsync(&buf, B * n * sizeof(double2), s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dc, hc.size() * 8, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dc, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, plain, 8ull * B * L * n, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // hc is a host vector
     if (e != cudaSuccess) return status_from(e);
-    r = ntt_inverse(c, tmp, tmp, B, 0, L, false, s);
+    int r = ntt_inverse(c, tmp, tmp, B, 0, L, false, s);
     if (r == TB_OK) {
         TraceScope ts("ckks_decode", s);
         ckks_compose<<<grid_for(B * n, 128), 128, 0, s>>>(tmp, buf, c.d_mods, dc, dc + 2 * L, dc + 2 * L + L * L,
                                                           dc + 2 * L + L * L + L, L, c.logn, 1.0 / scale, B);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) r = status_from(e);
+    }
+    cudaFreeAsync(tmp, s);
+    cudaFreeAsync(dc, s);
+    return r;
+}
+
+static int decode_checks(const Context &c, int L, const uint64_t *plain, double scale, const double *values) {
+    if (c.scheme != SCHEME_CKKS) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
+    if (L < 1 || L > (int)c.chain.size() || L + 1 > MAXW) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level");
+    if (!(scale > 0) || (int)std::log2(scale) >= total_bits(c, L))
+        return set_error(TB_ERR_INVALID_ARGUMENT, "scale out of bounds");
+    if (!plain || !values) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    return TB_OK;
+}
+
+// plaintexts [B][L][N] (NTT form) -> slot values [B][ostride] complex (N/2 used).
+int ckks_decode(Context &c, int L, const uint64_t *plain, double scale, double *values, uint64_t ostride, uint64_t B,
+                cudaStream_t s) {
+    int r = decode_checks(c, L, plain, scale, values);
+    if (r != TB_OK || !B) return r;
+    const uint32_t n = c.n;
+    if (!ostride) ostride = n / 2;
+    const uint32_t *map = nullptr;
+    double2 *roots, *iroots;
+    r = slot_map(c, &map);
+    if (r == TB_OK) r = ckks_tables(c, &roots, &iroots);
+    if (r != TB_OK) return r;
+    ensure_pool_retains(c.device);
+    double2 *buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, B * n * sizeof(double2), s);
+    if (e != cudaSuccess) return status_from(e);
+    r = compose_level(c, L, plain, scale, buf, B, s);
+    if (r == TB_OK) {
+        TraceScope ts("ckks_decode", s);
         for (int st = 0; st < c.logn; st++)
             fft_fwd_stage<<<grid_for(B * n / 2, 256), 256, 0, s>>>(buf, roots, c.logn, st, B);
         ckks_gather<<<grid_for(B * n / 2, 256), 256, 0, s>>>(buf, (double2 *)values, ostride, map, c.logn, B);
         e = cudaGetLastError();
         if (e != cudaSuccess) r = status_from(e);
     }
-    cudaFreeAsync(tmp, s);
     cudaFreeAsync(buf, s);
-    cudaFreeAsync(dc, s);
+    return r;
+}
+
+// plaintexts [B][L][N] (NTT form) -> N real coefficients each, divided by scale
+// (CKKSEncoderCuda::decodePolynomialInternal, src/ckks_cuda.cu:983-1040).
+int ckks_decode_polynomial(Context &c, int L, const uint64_t *plain, double scale, double *values, uint64_t ostride,
+                           uint64_t B, cudaStream_t s) {
+    int r = decode_checks(c, L, plain, scale, values);
+    if (r != TB_OK || !B) return r;
+    const uint32_t n = c.n;
+    if (!ostride) ostride = n;
+    ensure_pool_retains(c.device);
+    double2 *buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, B * n * sizeof(double2), s);
+    if (e != cudaSuccess) return status_from(e);
+    r = compose_level(c, L, plain, scale, buf, B, s);
+    if (r == TB_OK) {
+        ckks_store_real<<<grid_for(B * n, 256), 256, 0, s>>>(buf, values, ostride, c.logn, B);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) r = status_from(e);
+    }
+    cudaFreeAsync(buf, s);
     return r;
 }
 

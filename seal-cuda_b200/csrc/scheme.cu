@@ -745,3 +745,104 @@ int add_plain(Context &c, int L, int negate, uint64_t *ct, uint64_t cstride, con
 }
 
 }  // namespace tb
+
+namespace tb {
+
+// ------------------------------------------------------------------ scalars, constants
+
+namespace {
+
+// out = a * scalar mod q_l over `size` polys of L limbs (kMultiplyPolyScalarCoeffmod).
+__global__ void scalar_mul_kernel(const uint64_t *__restrict__ a, uint64_t astride, uint64_t *__restrict__ out,
+                                  uint64_t ostride, uint64_t scalar, const Mod *__restrict__ mods, int L, int logn,
+                                  int size, uint64_t B) {
+    const uint64_t per = ((uint64_t)size * L) << logn;
+    const uint64_t total = B * per;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = w / per, r = w - b * per;
+        const Mod m = mods[(r >> logn) % L];
+        out[b * ostride + r] = mul_mod(reduce64(a[b * astride + r], m), reduce64(scalar, m), m);
+    }
+}
+
+// words mod t times scalar mod t.
+__global__ void scalar_mul_t_kernel(const uint64_t *__restrict__ a, uint64_t astride, uint64_t *__restrict__ out,
+                                    uint64_t ostride, uint64_t count, uint64_t scalar, Mod t, uint64_t B) {
+    const uint64_t total = B * count;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = w / count, i = w - b * count;
+        out[b * ostride + i] = mul_mod(reduce64(a[b * astride + i], t), reduce64(scalar, t), t);
+    }
+}
+
+constexpr int MAX_FILL_LIMBS = 64;
+struct LimbValues {
+    uint64_t v[MAX_FILL_LIMBS];
+};
+
+__global__ void fill_limbs_kernel(uint64_t *__restrict__ out, LimbValues vals, int L, int logn, uint64_t B) {
+    const uint64_t total = (B * L) << logn;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)
+        out[w] = vals.v[(w >> logn) % L];
+}
+
+}  // namespace
+
+int multiply_scalar(Context &c, int L, int size, const uint64_t *a, uint64_t astride, uint64_t scalar, uint64_t *out,
+                    uint64_t ostride, uint64_t B, cudaStream_t s) {
+    if (L < 1 || L > (int)c.table_moduli.size() || size < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level or size");
+    if (!a || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!B) return TB_OK;
+    const uint64_t per = ((uint64_t)size * L) << c.logn;
+    if (!astride) astride = per;
+    if (!ostride) ostride = per;
+    TraceScope ts("multiply_scalar", s);
+    scalar_mul_kernel<<<grid_for(B * per, 256), 256, 0, s>>>(a, astride, out, ostride, scalar, c.d_mods, L, c.logn,
+                                                             size, B);
+    return status_from(cudaGetLastError());
+}
+
+int plain_multiply_scalar(Context &c, const uint64_t *a, uint64_t astride, uint64_t count, uint64_t scalar,
+                          uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s) {
+    if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
+    if (!a || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!B || !count) return TB_OK;
+    if (!astride) astride = count;
+    if (!ostride) ostride = count;
+    TraceScope ts("multiply_scalar", s);
+    scalar_mul_t_kernel<<<grid_for(B * count, 256), 256, 0, s>>>(a, astride, out, ostride, count, scalar, c.t_mod, B);
+    return status_from(cudaGetLastError());
+}
+
+// Lift `B` plaintexts mod t to level L (centred: values >= (t+1)/2 become value - t
+// mod q_l) and transform them: EvaluatorCuda::transformToNttInplace(Plaintext)
+// (src/evaluator_cuda.cu:1869-1935). Output [B][L][N], NTT form.
+int plain_to_ntt(Context &c, int L, const uint64_t *plain, uint64_t pstride, uint32_t pcount, uint64_t *out,
+                 uint64_t B, cudaStream_t s) {
+    if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV) return set_error(TB_ERR_UNSUPPORTED, "unsupported scheme");
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level");
+    if (pcount > c.n) return set_error(TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+    if (!plain || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!B) return TB_OK;
+    if (!pstride) pstride = pcount;
+    const RnsLevel &lv = c.levels[L];
+    if (!lv.d_consts) return set_error(TB_ERR_UNSUPPORTED, "plain modulus not coprime to q");
+    const uint64_t pl = (uint64_t)L * c.n;
+    TraceScope ts("plain_to_ntt", s);
+    plain_lift_kernel<<<grid_for(B * pl, 256), 256, 0, s>>>(plain, pstride, pcount, out, c.d_mods, lv.d_consts,
+                                                            lv.off, c.t, L, c.logn, B);
+    return status_from(transform<true>(c, out, B, 0, L, false, s));
+}
+
+// Every coefficient of limb l of each of B plaintexts [L][N] set to vals[l].
+int fill_limbs(Context &c, int L, const uint64_t *vals, uint64_t *out, uint64_t B, cudaStream_t s) {
+    if (L < 1 || L > (int)c.chain.size() || L > MAX_FILL_LIMBS) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level");
+    if (!out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!B) return TB_OK;
+    LimbValues lv{};
+    for (int l = 0; l < L; l++) lv.v[l] = vals[l];
+    fill_limbs_kernel<<<grid_for((B * L) << c.logn, 256), 256, 0, s>>>(out, lv, L, c.logn, B);
+    return status_from(cudaGetLastError());
+}
+
+}  // namespace tb

@@ -126,3 +126,44 @@ def test_batched_ckks_evaluation_decodes_to_the_product():
         assert np.abs(got[b] - exact).max() < 2.0 ** -14, b
         ref_dec = codec.decode(_host(ph)[b], new_scale)
         assert np.abs(got[b] - ref_dec).max() < 2.0 ** -20, b
+
+
+def _cround(x):
+    """C round(): halves away from zero (Python's round() rounds halves to even)."""
+    import math
+    f = math.floor(x)
+    d = x - f
+    return int(f + 1) if (d > 0.5 or (d == 0.5 and x > 0)) else int(f)
+
+
+def test_constant_and_coefficient_encoders():
+    """Constant encoders write round(value*scale) (or the integer) mod q_l into every
+    NTT coefficient (src/ckks.cpp:279-440), negative values negated mod q; the
+    coefficient encoder is exact after an inverse NTT and round-trips through
+    decode_polynomial."""
+    orc = Oracle("orc")
+    n = 4096
+    moduli = orc.coeff_modulus_create(n, [60, 40, 40, 60])
+    L = len(moduli) - 1
+    ctx = tb_capi.Context(2, n, moduli)
+    plain = torch.empty((L, n), dtype=torch.int64, device="cuda")
+    for value, scale in [(-1.5, 2.0 ** 40), (0.3, 2.0 ** 30), (12345.678, 2.0 ** 60)]:
+        ctx("ckks_encode_double", L, value, scale, plain, None)
+        c = _cround(value * scale)
+        exp = np.array([[c % q] * n for q in moduli[:L]], np.uint64)
+        assert np.array_equal(_host(plain), exp), (value, scale)
+    for value in [-7, 0, 2 ** 40 + 3]:
+        ctx("ckks_encode_int64", L, value, plain, None)
+        exp = np.array([[((value + q) % 2 ** 64 if value < 0 else value) % q] * n for q in moduli[:L]], np.uint64)
+        assert np.array_equal(_host(plain), exp), value
+    rng = np.random.default_rng(21)
+    coeffs = rng.uniform(-1000, 1000, (2, n))
+    pp = torch.empty((2, L, n), dtype=torch.int64, device="cuda")
+    ctx("ckks_encode_polynomial", L, torch.from_numpy(coeffs).cuda(), 0, n, 2.0 ** 40, pp, 2, None)
+    out = torch.empty((2, n), dtype=torch.float64, device="cuda")
+    ctx("ckks_decode_polynomial", L, pp, 2.0 ** 40, out, 0, 2, None)
+    assert np.abs(out.cpu().numpy() - coeffs).max() < 2.0 ** -25
+    raw = _host(pp)[0]
+    coef = np.stack([orc.ntt_inverse(12, q, raw[l].copy()) for l, q in enumerate(moduli[:L])])
+    exp = np.array([[_cround(x * 2.0 ** 40) % q for x in coeffs[0]] for q in moduli[:L]], np.uint64)
+    assert np.array_equal(coef, exp)
