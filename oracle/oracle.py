@@ -82,6 +82,8 @@ class Oracle:
             bind("poly_mul_scalar", None, [_u64, _c.c_int, _sz, _u64, _c.c_uint64, _u64])
             bind("ntt_forward_rns", _c.c_int, [_c.c_int, _u64, _c.c_int, _u64, _c.c_int])
             bind("ntt_inverse_rns", _c.c_int, [_c.c_int, _u64, _c.c_int, _u64, _c.c_int])
+        if kind == "ref":
+            bind("parms_id", _c.c_int, [_c.c_int, _sz, _u64, _c.c_int, _c.c_uint64, _u64])
 
     # ------------------------------------------------------------ primitives
     def ntt_tables(self, logn, q):
@@ -151,6 +153,13 @@ class Oracle:
         out = np.zeros(len(bits), np.uint64)
         if self._f["coeff_modulus_create"](n, _arr(bits, np.int32), len(bits), out):
             raise ValueError("cannot create coeff modulus")
+        return [int(x) for x in out]
+
+    def parms_id(self, scheme, n, moduli, t):
+        """EncryptionParameters::parmsID of the compiled reference (kind "ref" only)."""
+        out = np.zeros(4, np.uint64)
+        if self._f["parms_id"](scheme, n, _arr(moduli), len(moduli), t, out):
+            raise ValueError("invalid parameters")
         return [int(x) for x in out]
 
     def plain_modulus_batching(self, n, bits):

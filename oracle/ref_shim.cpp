@@ -124,6 +124,23 @@ int ref_coeff_modulus_create(size_t n, const int *bits, int count, uint64_t *out
     }
 }
 
+// EncryptionParameters::parmsID of (scheme, n, moduli, t).
+int ref_parms_id(int scheme, size_t n, const uint64_t *moduli, int count, uint64_t t, uint64_t *out4) {
+    try {
+        EncryptionParameters p(static_cast<SchemeType>(scheme));
+        p.setPolyModulusDegree(n);
+        std::vector<Modulus> q;
+        for (int i = 0; i < count; i++) q.emplace_back(moduli[i]);
+        p.setCoeffModulus(q);
+        if (t) p.setPlainModulus(t);
+        const auto &id = p.parmsID();
+        for (int i = 0; i < 4; i++) out4[i] = id[i];
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
 int ref_plain_modulus_batching(size_t n, int bits, uint64_t *out) {
     try {
         *out = PlainModulus::Batching(n, bits).value();

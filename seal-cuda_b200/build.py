@@ -82,12 +82,13 @@ def build_pytroy(verbose=False):
     ext = sysconfig.get_config_var("EXT_SUFFIX")
     out = os.path.join(LIB, "pytroy" + ext)
     srcs = [binder] + sorted(glob.glob(os.path.join(src_dir, "*.cpp")))
-    deps = srcs + glob.glob(os.path.join(src_dir, "*.hpp")) + [os.path.join(ROOT, "include", "troy_b200.h"), LIBNAME]
+    deps = srcs + glob.glob(os.path.join(src_dir, "*.hpp")) + [os.path.join(ROOT, "include", "troy_b200.h"), LIBNAME,
+                                                                os.path.join(CSRC, "hostmath.hpp")]
     if not _stale(out, deps):
         return out
     cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
            "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
-           "-I" + os.path.join(ROOT, "include"), "-I" + src_dir, "-I/usr/local/cuda/include"] + srcs + \
+           "-I" + os.path.join(ROOT, "include"), "-I" + src_dir, "-I" + CSRC, "-I/usr/local/cuda/include"] + srcs + \
           ["-o", out, "-L" + LIB, "-ltroy_b200", "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart"]
     if verbose:
         print(" ".join(cmd))

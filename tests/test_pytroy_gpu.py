@@ -1,0 +1,422 @@
+"""The `pytroy` module (troy's Python surface over this library) on the GPU.
+
+With a seeded Blake2xbPRNGFactory every key, encryption and evaluation result must
+be word-identical to the reference's (golden fixtures made by the reference,
+tests/golden/gen_golden.py); the rest of the evaluator surface is checked by
+decryption against plaintext arithmetic, in the style of the reference's own
+evaluator tests (test/evaluator_cuda.cu). Overloads are called as the reference
+module registers them (e.g. the returning mod_switch_to takes the parms_id first)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+pytroy = pytest.importorskip("pytroy")
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SEED = [int(x) for x in range(101, 109)]
+S = pytroy.SchemeType
+
+
+def _setup(scheme, n, moduli, t, seeded=True):
+    p = pytroy.EncryptionParameters(scheme)
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus([pytroy.Modulus(int(q)) for q in moduli])
+    if t:
+        p.set_plain_modulus(int(t))
+    if seeded:
+        p.set_random_generator(pytroy.Blake2xbPRNGFactory(SEED))
+    ctx = pytroy.SEALContext(p, True, pytroy.SecurityLevel.none)
+    assert ctx.parameters_set(), ctx.parameter_error_name()
+    return ctx
+
+
+def _words(x):
+    return np.asarray(x.data(), np.uint64)
+
+
+@pytest.mark.parametrize("prefix,scheme", [("bfv_", S.bfv), ("bgv_", S.bgv)])
+def test_seeded_chain_matches_reference_words(prefix, scheme):
+    z = np.load(os.path.join(G, "sessions_n64.npz"))
+    p = prefix
+    n = 64
+    ctx = _setup(scheme, n, z[p + "moduli"], z[p + "t"][0])
+    keygen = pytroy.KeyGenerator(ctx)
+    assert np.array_equal(_words(keygen.secret_key()), z[p + "sk"].reshape(-1))
+    pk = keygen.create_public_key()
+    assert np.array_equal(_words(pk), z[p + "pk"].reshape(-1))
+    rlk = keygen.create_relin_keys()
+    assert np.array_equal(np.asarray(rlk.data(0), np.uint64), z[p + "rlk"].reshape(-1))
+    elt = int(z[p + "elt"][0])
+    gk = keygen.create_galois_keys([1])
+    assert gk.has_key(elt)
+    assert np.array_equal(np.asarray(gk.data(elt), np.uint64), z[p + "gk"].reshape(-1))
+    enc = pytroy.BatchEncoder(ctx)
+    pa = enc.encode(z[p + "a"])
+    assert np.array_equal(_words(pa), z[p + "plain_a"])
+    encryptor = pytroy.Encryptor(ctx, pk)
+    ea = encryptor.encrypt(pa)
+    eb = encryptor.encrypt(enc.encode(z[p + "b"]))
+    assert np.array_equal(_words(ea), z[p + "enc_a"].reshape(-1))
+    assert np.array_equal(_words(eb), z[p + "enc_b"].reshape(-1))
+    ev = pytroy.Evaluator(ctx)
+    m = ev.multiply(ea, eb)
+    assert m.size() == 3 and np.array_equal(_words(m), z[p + "mul"].reshape(-1))
+    ev.relinearize_inplace(m, rlk)
+    assert m.size() == 2 and np.array_equal(_words(m), z[p + "relin"].reshape(-1))
+    r = ev.rotate_rows(m, 1, gk)
+    assert np.array_equal(_words(r), z[p + "rot"].reshape(-1))
+    assert r.correction_factor() == int(z[p + "correction"][0])
+    ms = ev.mod_switch_to_next(r)
+    assert np.array_equal(_words(ms), z[p + "modswitch"].reshape(-1))
+    dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    assert np.array_equal(enc.decode(dec.decrypt(r)), z[p + "dec"])
+    t = int(z[p + "t"][0])
+    exp = (z[p + "a"].astype(object) * z[p + "b"].astype(object)) % t
+    half = n // 2
+    exp = np.concatenate([np.roll(exp[:half], -1), np.roll(exp[half:], -1)]).astype(np.uint64)
+    assert np.array_equal(enc.decode(dec.decrypt(ms)), exp)
+
+
+def test_ckks_seeded_chain_matches_reference():
+    z = np.load(os.path.join(G, "sessions_n64.npz"))
+    p = "ckks_"
+    n = 64
+    ctx = _setup(S.ckks, n, z[p + "moduli"], 0)
+    keygen = pytroy.KeyGenerator(ctx)
+    assert np.array_equal(_words(keygen.secret_key()), z[p + "sk"].reshape(-1))
+    pk = keygen.create_public_key()
+    assert np.array_equal(_words(pk), z[p + "pk"].reshape(-1))
+    rlk = keygen.create_relin_keys()
+    elt = int(z[p + "elt"][0])
+    gk = keygen.create_galois_keys([1])
+    assert np.array_equal(np.asarray(gk.data(elt), np.uint64), z[p + "gk"].reshape(-1))
+    enc = pytroy.CKKSEncoder(ctx)
+    scale = float(z[p + "scale"][0])
+    pv = enc.encode(z[p + "v"], scale)
+    assert np.array_equal(_words(pv), z[p + "plain_v"].reshape(-1))
+    encryptor = pytroy.Encryptor(ctx, pk)
+    ea = encryptor.encrypt(pv)
+    eb = encryptor.encrypt(enc.encode(z[p + "w"], scale))
+    assert np.array_equal(_words(ea), z[p + "enc_a"].reshape(-1))
+    assert np.array_equal(_words(eb), z[p + "enc_b"].reshape(-1))
+    ev = pytroy.Evaluator(ctx)
+    m = ev.multiply(ea, eb)
+    assert np.array_equal(_words(m), z[p + "mul"].reshape(-1))
+    ev.relinearize_inplace(m, rlk)
+    ev.rescale_to_next_inplace(m)
+    assert np.array_equal(_words(m), z[p + "rescale"].reshape(-1))
+    assert m.scale() == pytest.approx(scale * scale / int(z[p + "moduli"][-2]), rel=1e-15)
+    r = ev.rotate_vector(m, 1, gk)
+    assert np.array_equal(_words(r), z[p + "rot"].reshape(-1))
+    got = enc.decode(pytroy.Decryptor(ctx, keygen.secret_key()).decrypt(r))
+    assert np.abs(got - z[p + "dec"]).max() < 2.0 ** -20
+
+
+@pytest.fixture(scope="module")
+def bfv():
+    n = 8192
+    t = pytroy.PlainModulus.batching(n, 20)
+    p = pytroy.EncryptionParameters(S.bfv)
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus(pytroy.CoeffModulus.create(n, [43, 43, 44, 44, 44]))
+    p.set_plain_modulus(t)
+    ctx = pytroy.SEALContext(p)
+    keygen = pytroy.KeyGenerator(ctx)
+    ns = type("NS", (), {})()
+    ns.ctx, ns.t, ns.n = ctx, t.value(), n
+    ns.keygen = keygen
+    ns.enc = pytroy.BatchEncoder(ctx)
+    ns.encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    ns.dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    ns.ev = pytroy.Evaluator(ctx)
+    ns.rlk = keygen.create_relin_keys()
+    ns.gk = keygen.create_galois_keys()
+    ns.rng = np.random.default_rng(5)
+    return ns
+
+
+def _rand(ns):
+    return ns.rng.integers(0, ns.t, ns.n, dtype=np.uint64)
+
+
+def _enc(ns, v):
+    return ns.encryptor.encrypt(ns.enc.encode(v))
+
+
+def _dec(ns, c):
+    return ns.enc.decode(ns.dec.decrypt(c))
+
+
+def _mul(ns, a, b):
+    return ((a.astype(object) * b.astype(object)) % ns.t).astype(np.uint64)
+
+
+def test_bfv_evaluator_surface(bfv):
+    ns = bfv
+    t = ns.t
+    a, b, c = _rand(ns), _rand(ns), _rand(ns)
+    ca, cb, cc = _enc(ns, a), _enc(ns, b), _enc(ns, c)
+    ev = ns.ev
+    assert np.array_equal(_dec(ns, ev.add(ca, cb)), (a + b) % t)
+    assert np.array_equal(_dec(ns, ev.sub(ca, cb)), (a + t - b) % t)
+    assert np.array_equal(_dec(ns, ev.negate(ca)), (t - a) % t)
+    assert np.array_equal(_dec(ns, ev.add_many([ca, cb, cc])), (a + b + c) % t)
+    assert np.array_equal(_dec(ns, ev.add_plain(ca, ns.enc.encode(b))), (a + b) % t)
+    assert np.array_equal(_dec(ns, ev.sub_plain(ca, ns.enc.encode(b))), (a + t - b) % t)
+    assert np.array_equal(_dec(ns, ev.multiply_plain(ca, ns.enc.encode(b))), _mul(ns, a, b))
+    sq = ev.square(ca)
+    assert sq.size() == 3
+    ev.relinearize_inplace(sq, ns.rlk)
+    assert np.array_equal(_dec(ns, sq), _mul(ns, a, a))
+    assert np.array_equal(_dec(ns, ev.exponentiate(ca, 3, ns.rlk)), _mul(ns, _mul(ns, a, a), a))
+    assert np.array_equal(_dec(ns, ev.multiply_many([ca, cb, cc], ns.rlk)), _mul(ns, _mul(ns, a, b), c))
+    # NTT-form plaintext multiply on an NTT-form ciphertext
+    pb = ev.transform_to_ntt(ns.enc.encode(b), ns.ctx.first_parms_id())
+    assert pb.is_ntt_form()
+    cn = ev.transform_to_ntt(ca)
+    assert cn.is_ntt_form()
+    ev.multiply_plain_inplace(cn, pb)
+    ev.transform_from_ntt_inplace(cn)
+    assert np.array_equal(_dec(ns, cn), _mul(ns, a, b))
+    # rotations: direct key, NAF decomposition (3 = 4 - 1, -5 = -1 - 4), columns, and
+    # the rotate_rows(cipher, keys) overload that swaps the columns
+    half = ns.n // 2
+    rows = lambda v, k: np.concatenate([np.roll(v[:half], -k), np.roll(v[half:], -k)])
+    cols = lambda v: np.concatenate([v[half:], v[:half]])
+    assert np.array_equal(_dec(ns, ev.rotate_rows(ca, 1, ns.gk)), rows(a, 1))
+    assert np.array_equal(_dec(ns, ev.rotate_rows(ca, 3, ns.gk)), rows(a, 3))
+    assert np.array_equal(_dec(ns, ev.rotate_rows(ca, -5, ns.gk)), rows(a, -5))
+    rc = pytroy.Ciphertext()
+    ev.rotate_columns(ca, ns.gk, rc)
+    assert np.array_equal(_dec(ns, rc), cols(a))
+    assert np.array_equal(_dec(ns, ev.rotate_rows(ca, ns.gk)), cols(a))
+    # modulus switching down the chain
+    last = ns.ctx.last_parms_id()
+    low = ev.mod_switch_to(last, ca)
+    assert low.parms_id() == last and low.coeff_modulus_size() == 1
+    assert np.array_equal(_dec(ns, low), a)
+    with pytest.raises(ValueError):
+        ev.mod_switch_to_next(low)
+    with pytest.raises(ValueError):
+        ev.rescale_to_next(ca)
+    # symmetric encryption and signed values
+    sym = pytroy.Encryptor(ns.ctx, ns.keygen.secret_key())
+    signed = ns.rng.integers(-(t // 2), t // 2, ns.n, dtype=np.int64)
+    cs = sym.encrypt_symmetric(ns.enc.encode_int64(signed))
+    assert np.array_equal(ns.enc.decode_int64(ns.dec.decrypt(cs)), signed)
+    z = ns.encryptor.encrypt_zero()
+    assert np.array_equal(_dec(ns, ev.add(ca, z)), a)
+
+
+def test_bgv_correction_factor_balancing():
+    n = 8192
+    p = pytroy.EncryptionParameters(S.bgv)
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus(pytroy.CoeffModulus.create(n, [43, 43, 44, 44, 44]))
+    t = pytroy.PlainModulus.batching(n, 20).value()
+    p.set_plain_modulus(t)
+    ctx = pytroy.SEALContext(p)
+    keygen = pytroy.KeyGenerator(ctx)
+    enc = pytroy.BatchEncoder(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    ev = pytroy.Evaluator(ctx)
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, t, n, dtype=np.uint64)
+    b = rng.integers(0, t, n, dtype=np.uint64)
+    ca = ev.mod_switch_to_next(encryptor.encrypt(enc.encode(a)))
+    assert ca.correction_factor() != 1
+    cb = encryptor.encrypt_zero(ca.parms_id())
+    ev.add_plain_inplace(cb, enc.encode(b))
+    assert cb.correction_factor() == 1
+    s = ev.add(ca, cb)
+    assert np.array_equal(enc.decode(dec.decrypt(s)), (a + b) % t)
+    d = ev.sub(ca, cb)
+    assert np.array_equal(enc.decode(dec.decrypt(d)), (a + t - b) % t)
+    ev.add_plain_inplace(ca, enc.encode(b))
+    assert np.array_equal(enc.decode(dec.decrypt(ca)), (a + b) % t)
+
+
+def test_ckks_encoder_and_evaluator_surface():
+    n = 8192
+    p = pytroy.EncryptionParameters(S.ckks)
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus(pytroy.CoeffModulus.create(n, [60, 40, 40, 60]))
+    ctx = pytroy.SEALContext(p)
+    keygen = pytroy.KeyGenerator(ctx)
+    enc = pytroy.CKKSEncoder(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    ev = pytroy.Evaluator(ctx)
+    rlk = keygen.create_relin_keys()
+    gk = keygen.create_galois_keys()
+    scale = 2.0 ** 40
+    rng = np.random.default_rng(13)
+    slots = n // 2
+    v = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    w = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    cv, cw = encryptor.encrypt(enc.encode(v, scale)), encryptor.encrypt(enc.encode(w, scale))
+    d = lambda c: enc.decode(dec.decrypt(c))
+    tol = 2.0 ** -20
+    assert np.abs(d(ev.add(cv, cw)) - (v + w)).max() < tol
+    assert np.abs(d(ev.sub(cv, cw)) - (v - w)).max() < tol
+    assert np.abs(d(ev.negate(cv)) + v).max() < tol
+    m = ev.multiply(cv, cw)
+    ev.relinearize_inplace(m, rlk)
+    ev.rescale_to_next_inplace(m)
+    assert np.abs(d(m) - v * w).max() < 2.0 ** -15
+    assert np.abs(d(ev.rotate_vector(cv, 3, gk)) - np.roll(v, -3)).max() < tol
+    assert np.abs(d(ev.rotate_vector(cv, -7, gk)) - np.roll(v, 7)).max() < tol
+    assert np.abs(d(ev.complex_conjugate(cv, gk)) - np.conj(v)).max() < tol
+    pc = enc.encode(complex(0.25, -0.5), scale)  # a complex constant fills every slot
+    assert np.abs(d(ev.add_plain(cv, pc)) - (v + complex(0.25, -0.5))).max() < tol
+    # a bare float resolves to the complex-constant overload: every slot carries it
+    pd = pytroy.Plaintext()
+    enc.encode(-1.5, scale, pd)
+    assert np.abs(enc.decode(pd) + 1.5).max() < tol
+    coeffs = rng.uniform(-100, 100, n)
+    pp = enc.encode_polynomial(coeffs, scale)
+    assert np.abs(enc.decode_polynomial(pp) - coeffs).max() < 2.0 ** -20
+    mp = ev.multiply_plain(cv, enc.encode(w, scale))
+    ev.rescale_to_next_inplace(mp)
+    assert np.abs(d(mp) - v * w).max() < 2.0 ** -15
+    # mod switch (drop a prime, keep the scale) for ciphertexts and plaintexts
+    low = ev.mod_switch_to_next(cv)
+    assert low.coeff_modulus_size() == 2 and low.scale() == scale
+    assert np.abs(d(low) - v).max() < tol
+    pl = ev.mod_switch_to_next(enc.encode(w, scale))
+    assert pl.parms_id() == low.parms_id()
+    assert np.abs(d(ev.add_plain(low, pl)) - (v + w)).max() < tol
+    with pytest.raises(ValueError):
+        ev.add(cv, low)
+
+
+def _parse_ct(b, off=0):
+    """Fields of the reference's ciphertext wire format (src/ciphertext_cuda.cu:8-34)."""
+    u = lambda o: int(np.frombuffer(b, np.uint64, 1, o)[0])
+    pid = [u(off + 8 * i) for i in range(4)]
+    off += 32
+    ntt = b[off] != 0
+    off += 1
+    size, n, L = u(off), u(off + 8), u(off + 16)
+    scale = float(np.frombuffer(b, np.float64, 1, off + 24)[0])
+    cf, seed = u(off + 32), u(off + 40)
+    terms = b[off + 48] != 0
+    off += 49
+    count = u(off)
+    off += 8
+    data = np.frombuffer(b, np.uint64, count, off)
+    return dict(parms_id=pid, ntt=ntt, size=size, n=n, L=L, scale=scale, cf=cf, seed=seed, terms=terms,
+                data=data), off + 8 * count
+
+
+def test_serialization_wire_format_and_round_trip():
+    z = np.load(os.path.join(G, "sessions_n64.npz"))
+    p = "bfv_"
+    n = 64
+    ctx = _setup(S.bfv, n, z[p + "moduli"], z[p + "t"][0])
+    K = len(z[p + "moduli"])
+    keygen = pytroy.KeyGenerator(ctx)
+    pk = keygen.create_public_key()
+    rlk = keygen.create_relin_keys()
+    gk = keygen.create_galois_keys([1])
+    enc = pytroy.BatchEncoder(ctx)
+    ev = pytroy.Evaluator(ctx)
+    ct = pytroy.Encryptor(ctx, pk).encrypt(enc.encode(z[p + "a"]))
+    b = ct.save()
+    f, end = _parse_ct(b)
+    assert end == len(b)
+    assert f["parms_id"] == ctx.first_parms_id() and not f["ntt"] and f["size"] == 2 and f["n"] == n
+    assert f["L"] == K - 1 and f["scale"] == 1.0 and f["cf"] == 1 and f["seed"] == 0 and not f["terms"]
+    assert np.array_equal(f["data"], z[p + "enc_a"].reshape(-1))
+    c2 = pytroy.Ciphertext()
+    c2.load(b)
+    assert np.array_equal(_words(c2), _words(ct)) and c2.parms_id() == ct.parms_id()
+    c3 = pytroy.Ciphertext()
+    c3.load(b, ctx)
+    assert np.array_equal(_words(c3), _words(ct))
+    # public key = one NTT-form ciphertext at the key level
+    f, end = _parse_ct(pk.save())
+    assert f["ntt"] and f["L"] == K and np.array_equal(f["data"], z[p + "pk"].reshape(-1))
+    # secret key = plaintext (parms_id, coeff_count, scale, words)
+    sb = keygen.secret_key().save()
+    assert int(np.frombuffer(sb, np.uint64, 1, 32)[0]) == K * n
+    assert np.array_equal(np.frombuffer(sb, np.uint64, K * n, 56), z[p + "sk"].reshape(-1))
+    # key-switching keys: parms_id, slot count, per slot digit count and digits
+    rb = rlk.save()
+    assert int(np.frombuffer(rb, np.uint64, 1, 32)[0]) == 1
+    assert int(np.frombuffer(rb, np.uint64, 1, 40)[0]) == K - 1
+    off, digits = 48, []
+    for _ in range(K - 1):
+        f, off = _parse_ct(rb, off)
+        digits.append(f["data"])
+    assert off == len(rb) and np.array_equal(np.concatenate(digits), z[p + "rlk"].reshape(-1))
+    gb = gk.save()
+    assert int(np.frombuffer(gb, np.uint64, 1, 32)[0]) == n  # N slots, as the reference sizes them
+    g2 = pytroy.GaloisKeys()
+    g2.load(gb)
+    r2 = pytroy.RelinKeys()
+    r2.load(rb)
+    m = ev.multiply(ct, ct)
+    ev.relinearize_inplace(m, r2)
+    assert np.array_equal(_words(ev.rotate_rows(m, 1, g2)), _words(ev.rotate_rows(m, 1, gk)))
+    # termed ciphertexts: only the listed coefficients of c0 travel
+    ids = np.array([0, 5, 17, 63], np.uint64)
+    tb = ct.save_terms(ev, ids)
+    ct_t = pytroy.Ciphertext()
+    ct_t.load_terms(tb, ev, ids)
+    w, wt = _words(ct).reshape(2, K - 1, n), _words(ct_t).reshape(2, K - 1, n)
+    assert np.array_equal(wt[1], w[1])
+    assert np.array_equal(wt[0][:, ids.astype(int)], w[0][:, ids.astype(int)])
+    mask = np.ones(n, bool)
+    mask[ids.astype(int)] = False
+    assert not wt[0][:, mask].any()
+
+
+def test_two_party_flow_like_the_reference_binder_test():
+    """binder/test.py of the reference: Alice keeps the secret key, Bob evaluates on
+    bytes only, in a context of his own."""
+    n, bits = 1 << 14, [40] * 6
+
+    def params():
+        p = pytroy.EncryptionParameters(S.ckks)
+        p.set_poly_modulus_degree(n)
+        p.set_coeff_modulus(pytroy.CoeffModulus.create(n, bits))
+        return p
+
+    pytroy.initialize_kernel()
+    a_ctx = pytroy.SEALContext(params())
+    a_enc = pytroy.CKKSEncoder(a_ctx)
+    keygen = pytroy.KeyGenerator(a_ctx)
+    pk = keygen.create_public_key()
+    rlk = keygen.create_relin_keys()
+    gk = keygen.create_galois_keys([1])
+    rlk.load(rlk.save())
+    keys = (pk.save(), rlk.save(), gk.save())
+    encryptor = pytroy.Encryptor(a_ctx, pk)
+    c1, c2 = pytroy.Ciphertext(), pytroy.Ciphertext()
+    p1, p2 = pytroy.Plaintext(), pytroy.Plaintext()
+    a_enc.encode([1, 2, 3, 4], 1 << 40, p1)
+    a_enc.encode([0.5, 0.6, 0.7, 0.8], 1 << 40, p2)
+    encryptor.encrypt(p1, c1)
+    encryptor.encrypt(p2, c2)
+
+    b_ctx = pytroy.SEALContext(params())
+    b_pk, b_rlk, b_gk = pytroy.PublicKey(), pytroy.RelinKeys(), pytroy.GaloisKeys()
+    b_pk.load(keys[0])
+    b_rlk.load(keys[1])
+    b_gk.load(keys[2])
+    b_ev = pytroy.Evaluator(b_ctx)
+    x, y = pytroy.Ciphertext(), pytroy.Ciphertext()
+    x.load(c1.save())
+    y.load(c2.save())
+    b_ev.multiply_inplace(x, y)
+    b_ev.relinearize_inplace(x, b_rlk)
+    b_ev.rescale_to_next_inplace(x)
+    b_ev.rotate_vector_inplace(x, 1, b_gk)
+    out = pytroy.Ciphertext()
+    out.load(x.save())
+    got = a_enc.decode(pytroy.Decryptor(a_ctx, keygen.secret_key()).decrypt(out))
+    assert np.abs(got[:3] - np.array([1.2, 2.1, 3.2])).max() < 1e-5
