@@ -310,6 +310,33 @@ int tb_multiply_scalar(tb_context *ctx, int L, int size, const uint64_t *a, uint
 int tb_plain_multiply_scalar(tb_context *ctx, const uint64_t *plain, uint64_t plain_stride, uint64_t count,
                              uint64_t scalar, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
 
+/*
+ * Sum of plaintext products in the NTT domain, the inner loop of the reference's
+ * matrix helpers (MatmulHelper::matmul: multiplyPlain then addInplace per output,
+ * app/LinearHelper.cuh:323-346) done as one pass: for each of `outputs` results o,
+ *   out[o] = sum_{k = term_offsets[o]} ^{term_offsets[o+1]-1} a[term_a[k]] (.) w[term_w[k]]
+ * where a[i] has `size` polynomials of L limbs (a_stride words apart), w[j] one
+ * polynomial of L limbs (w_stride apart), out[o] `size` polynomials (out_stride
+ * apart); strides 0 = packed. term_offsets / term_a / term_w are DEVICE arrays of
+ * uint32 (outputs+1, and one entry per term). Exact: canonical residues of the
+ * same sums the reference computes one product at a time.
+ */
+int tb_dyadic_accumulate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *w,
+                         uint64_t w_stride, uint64_t *out, uint64_t out_stride, const uint32_t *term_offsets,
+                         const uint32_t *term_a, const uint32_t *term_w, uint32_t outputs, void *stream);
+
+/*
+ * Weight plaintexts of the matrix helpers' coefficient encoding
+ * (MatmulHelper::encodeWeightSmall, app/LinearHelper.cuh:230-247) built on the device:
+ * `count` plaintexts of n words each. blocks is a DEVICE array of `count` records of
+ * 8 uint32: {source word offset (low, high), in, out, input block, output block,
+ * first row li, first column lj}; plaintext p takes rows li..li+block-1 and columns
+ * lj..lj+block-1 of the row-major in x out matrix at weights + offset, weight (i, j) at
+ * coefficient (j - lj) * input_block + input_block - 1 - (i - li), zeros elsewhere.
+ */
+int tb_matmul_encode_weights(tb_context *ctx, const uint64_t *weights, const uint32_t *blocks, uint64_t count,
+                             uint64_t *plain, void *stream);
+
 /* Element-wise ciphertext add / sub / negate over `size` polynomials at level L
    (kernel_util::kAddPolyCoeffmod / kSubPolyCoeffmod / kNegatePolyCoeffmod, src/kernelutils.cuh). */
 int tb_add(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *b,

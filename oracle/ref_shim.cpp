@@ -481,6 +481,41 @@ int ref_ct_multiply_plain_slots(void *h, int a, const uint64_t *slots, size_t co
     }
 }
 
+// The coefficient encoding of BatchEncoderCuda::encodePolynomial
+// (src/batchencoder_cuda.cu:124-144): count coefficients, each reduced mod t.
+static Plaintext poly_plain(Session *s, const uint64_t *coeffs, size_t count) {
+    const uint64_t t = s->parms->plainModulus().value();
+    Plaintext p(count);
+    for (size_t i = 0; i < count; i++) p.data()[i] = coeffs[i] % t;
+    return p;
+}
+
+// Encrypts BatchEncoder::encodePolynomial(coeffs) (coefficient encoding).
+int ref_ct_encrypt_poly(void *h, const uint64_t *coeffs, size_t count) {
+    auto *s = static_cast<Session *>(h);
+    try {
+        Plaintext p = poly_plain(s, coeffs, count);
+        Ciphertext c;
+        s->encryptor->encrypt(p, c);
+        return add_ct(s, std::move(c));
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Evaluator::multiplyPlain by encodePolynomial(coeffs).
+int ref_ct_multiply_plain_poly(void *h, int a, const uint64_t *coeffs, size_t count) {
+    auto *s = static_cast<Session *>(h);
+    try {
+        Plaintext p = poly_plain(s, coeffs, count);
+        Ciphertext c;
+        s->evaluator->multiplyPlain(s->cts.at(a), p, c);
+        return add_ct(s, std::move(c));
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_ct_add(void *h, int a, int b) {
     auto *s = static_cast<Session *>(h);
     try {

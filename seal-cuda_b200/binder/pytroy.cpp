@@ -12,6 +12,7 @@
 
 #include <sstream>
 
+#include "serving.hpp"
 #include "troy_b200.hpp"
 
 namespace py = pybind11;
@@ -495,4 +496,77 @@ PYBIND11_MODULE(pytroy, m) {
         .def("complex_conjugate", &E::complexConjugate)
         .def("complex_conjugate",
              [](const E &self, const C &c, const GK &k) { C r; self.complexConjugate(c, k, r); return r; });
+
+    // MatmulHelper (app/LinearHelper.cuh:197-452; binder.cu:700-760): coefficient-encoded
+    // vector x matrix products, the products of one call fused into one device pass.
+    auto check_len = [](const U64Array &a, std::size_t want, const char *what) {
+        if ((std::size_t)a.size() != want) throw std::invalid_argument(std::string(what) + " size incorrect.");
+    };
+    py::class_<MatmulHelper>(m, "MatmulHelper")
+        .def(py::init<std::size_t, std::size_t, std::size_t, std::size_t>())
+        .def_property_readonly("batch_block", [](const MatmulHelper &h) { return h.plan().batchBlock; })
+        .def_property_readonly("input_block", [](const MatmulHelper &h) { return h.plan().inputBlock; })
+        .def_property_readonly("output_block", [](const MatmulHelper &h) { return h.plan().outputBlock; })
+        .def("encode_weights",
+             [check_len](const MatmulHelper &h, const BatchEncoder &enc, U64Array w) {
+                 check_len(w, h.plan().in * h.plan().out, "Weight");
+                 return h.encodeWeights(enc, w.data());
+             })
+        .def("encode_inputs",
+             [check_len](const MatmulHelper &h, const BatchEncoder &enc, U64Array x) {
+                 check_len(x, h.plan().batch * h.plan().in, "Input");
+                 return h.encodeInputs(enc, x.data());
+             })
+        .def("encrypt_inputs",
+             [check_len](const MatmulHelper &h, const Encryptor &e, const BatchEncoder &enc, U64Array x) {
+                 check_len(x, h.plan().batch * h.plan().in, "Input");
+                 return h.encryptInputs(e, enc, x.data());
+             })
+        .def("matmul", &MatmulHelper::matmul)
+        .def("decrypt_outputs", [](const MatmulHelper &h, const BatchEncoder &enc, Decryptor &dec, const Cipher2d &c) {
+            return to_array(h.decryptOutputs(enc, dec, c));
+        });
+
+    // Continuous-batching server of single-row MatmulHelper products.
+    py::class_<MatmulServer>(m, "MatmulServer")
+        .def(py::init([](const SEALContext &ctx, std::size_t memory_budget, int slots, std::size_t max_wave_requests) {
+                 MatmulServer::Options o;
+                 o.memory_budget = memory_budget;
+                 o.slots = slots;
+                 o.max_wave_requests = max_wave_requests;
+                 return std::make_unique<MatmulServer>(ctx, o);
+             }),
+             py::arg("context"), py::arg("memory_budget") = std::size_t(8) << 30, py::arg("slots") = 3,
+             py::arg("max_wave_requests") = 256, py::keep_alive<1, 2>())
+        .def_static("now", &MatmulServer::now)
+        .def("submit",
+             [](MatmulServer &s, std::size_t in, std::size_t out, U64Array inputs, U64Array weights, double arrival) {
+                 if ((std::size_t)weights.size() != in * out) throw std::invalid_argument("Weight size incorrect.");
+                 return s.submit(in, out, inputs.data(), inputs.size(), weights.data(), arrival);
+             })
+        .def("step", &MatmulServer::step)
+        .def("drain", &MatmulServer::drain)
+        .def("idle", &MatmulServer::idle)
+        .def("queued", &MatmulServer::queued)
+        .def("result",
+             [](MatmulServer &s, std::uint64_t id) -> py::object {
+                 vector<uint64_t> out;
+                 double arrival = 0, done = 0;
+                 bool ok = false;
+                 if (!s.result(id, out, arrival, done, ok)) return py::none();
+                 return py::make_tuple(to_array(out), arrival, done, ok);
+             })
+        .def("release", &MatmulServer::release)
+        .def("inject_wave_failure", &MatmulServer::injectWaveFailure)
+        .def("stats", [](const MatmulServer &s) {
+            const auto &st = s.stats();
+            py::dict d;
+            d["submitted"] = st.submitted;
+            d["completed"] = st.completed;
+            d["failed"] = st.failed;
+            d["waves"] = st.waves;
+            d["peak_bytes"] = st.peak_bytes;
+            d["max_wave"] = st.max_wave;
+            return d;
+        });
 }

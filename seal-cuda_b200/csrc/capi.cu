@@ -64,6 +64,11 @@ int ckks_decode_polynomial(Context &c, int L, const uint64_t *plain, double scal
                            uint64_t B, cudaStream_t s);
 int ckks_encode_double(Context &c, int L, double value, double scale, uint64_t *out, cudaStream_t s);
 int ckks_encode_int64(Context &c, int L, int64_t value, uint64_t *out, cudaStream_t s);
+int matmul_encode_weights(Context &c, const uint64_t *weights, const uint32_t *blocks, uint64_t count, uint64_t *out,
+                          cudaStream_t s);
+int dyadic_accumulate(const Context &c, int L, int size, const uint64_t *a, uint64_t astride, const uint64_t *w,
+                      uint64_t wstride, uint64_t *out, uint64_t ostride, const uint32_t *off, const uint32_t *ia,
+                      const uint32_t *iw, uint32_t nout, cudaStream_t s);
 
 int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, uint64_t *out, uint64_t cstride_out,
                     int size, uint64_t B, cudaStream_t s);
@@ -342,6 +347,22 @@ int tb_plain_multiply_scalar(tb_context *ctx, const uint64_t *plain, uint64_t pl
                              uint64_t scalar, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
     return on_device(ctx, [&](tb::Context &c) {
         return tb::plain_multiply_scalar(c, plain, plain_stride, count, scalar, out, out_stride, batch, S(stream));
+    });
+}
+
+int tb_dyadic_accumulate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, const uint64_t *w,
+                         uint64_t w_stride, uint64_t *out, uint64_t out_stride, const uint32_t *term_offsets,
+                         const uint32_t *term_a, const uint32_t *term_w, uint32_t outputs, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::dyadic_accumulate(c, L, size, a, a_stride, w, w_stride, out, out_stride, term_offsets, term_a,
+                                     term_w, outputs, S(stream));
+    });
+}
+
+int tb_matmul_encode_weights(tb_context *ctx, const uint64_t *weights, const uint32_t *blocks, uint64_t count,
+                             uint64_t *plain, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::matmul_encode_weights(c, weights, blocks, count, plain, S(stream));
     });
 }
 

@@ -108,3 +108,59 @@ int tensor_product(const Context &c, int first, int L, const uint64_t *a, uint64
 }
 
 }  // namespace tb
+
+namespace tb {
+namespace {
+
+// out[o] = sum over terms k of output o of a[ia[k]] (.) w[iw[k]]: `size` polynomials
+// of L limbs each for a and out, one polynomial of L limbs for w (NTT domain).
+// Products are summed in 128 bits and reduced once per 63 terms, so any table
+// modulus (< 2^61) is safe; the result is canonical.
+__global__ void dyadic_accumulate_kernel(const uint64_t *__restrict__ a, uint64_t astride,
+                                         const uint64_t *__restrict__ w, uint64_t wstride, uint64_t *__restrict__ out,
+                                         uint64_t ostride, const uint32_t *__restrict__ off,
+                                         const uint32_t *__restrict__ ia, const uint32_t *__restrict__ iw,
+                                         const Mod *__restrict__ mods, int L, int logn, int size, uint32_t nout) {
+    const uint64_t n = 1ull << logn;
+    const uint64_t per = (uint64_t)size * L * n;
+    const uint64_t total = (uint64_t)nout * per;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total; x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t o = (uint32_t)(x / per);
+        const uint64_t r = x - (uint64_t)o * per;      // (poly, limb, coefficient) inside the output
+        const uint64_t lw = r % (L * n);                // (limb, coefficient) inside one polynomial
+        const Mod m = mods[lw >> logn];
+        U128 acc{0, 0};
+        uint64_t folded = 0;
+        int pending = 0;
+        const uint32_t k1 = off[o + 1];
+        for (uint32_t k = off[o]; k < k1; k++) {
+            mac128(acc, a[(uint64_t)ia[k] * astride + r], w[(uint64_t)iw[k] * wstride + lw]);
+            if (++pending == 63) {
+                folded = add_mod(folded, reduce128(acc.hi, acc.lo, m), m.value);
+                acc = U128{0, 0};
+                pending = 0;
+            }
+        }
+        out[(uint64_t)o * ostride + r] = add_mod(folded, reduce128(acc.hi, acc.lo, m), m.value);
+    }
+}
+
+}  // namespace
+
+int dyadic_accumulate(const Context &c, int L, int size, const uint64_t *a, uint64_t astride, const uint64_t *w,
+                      uint64_t wstride, uint64_t *out, uint64_t ostride, const uint32_t *off, const uint32_t *ia,
+                      const uint32_t *iw, uint32_t nout, cudaStream_t s) {
+    if (L < 1 || L > (int)c.table_moduli.size() || size < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "bad level or size");
+    if (!nout) return TB_OK;
+    if (!a || !w || !out || !off || !ia || !iw) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    const uint64_t pl = (uint64_t)L << c.logn;
+    if (!astride) astride = size * pl;
+    if (!wstride) wstride = pl;
+    if (!ostride) ostride = size * pl;
+    TraceScope ts("dyadic_accumulate", s);
+    dyadic_accumulate_kernel<<<grid_for((uint64_t)nout * size * pl, 256), 256, 0, s>>>(
+        a, astride, w, wstride, out, ostride, off, ia, iw, c.d_mods, L, c.logn, size, nout);
+    return status_from(cudaGetLastError());
+}
+
+}  // namespace tb

@@ -846,3 +846,44 @@ int fill_limbs(Context &c, int L, const uint64_t *vals, uint64_t *out, uint64_t 
 }
 
 }  // namespace tb
+
+namespace tb {
+namespace {
+
+// One weight plaintext of the matrix helpers' coefficient encoding
+// (MatmulHelper::encodeWeightSmall, app/LinearHelper.cuh:230-247): rows li.., columns
+// lj.. of a row-major in x out matrix at word offset src; coefficient
+// (j - lj) * ib + ib - 1 - (i - li) holds weight (i, j), all others are zero.
+struct WeightBlock {
+    uint64_t src;
+    uint32_t in, out, ib, ob, li, lj;
+};
+
+__global__ void weight_scatter_kernel(const uint64_t *__restrict__ weights, const WeightBlock *__restrict__ blocks,
+                                      uint64_t *__restrict__ out, int logn, uint64_t count) {
+    const uint32_t n = 1u << logn;
+    const uint64_t total = count << logn;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total; x += (uint64_t)gridDim.x * blockDim.x) {
+        const WeightBlock b = blocks[x >> logn];
+        const uint32_t r = (uint32_t)(x & (n - 1));
+        uint64_t v = 0;
+        const uint32_t jj = r / b.ib, ii = b.ib - 1 - (r - jj * b.ib);
+        const uint32_t i = b.li + ii, j = b.lj + jj;
+        if (jj < b.ob && i < b.in && j < b.out && i < b.li + b.ib) v = weights[b.src + (uint64_t)i * b.out + j];
+        out[x] = v;
+    }
+}
+
+}  // namespace
+
+int matmul_encode_weights(Context &c, const uint64_t *weights, const uint32_t *blocks, uint64_t count, uint64_t *out,
+                          cudaStream_t s) {
+    if (!count) return TB_OK;
+    if (!weights || !blocks || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    TraceScope ts("matmul_encode_weights", s);
+    weight_scatter_kernel<<<grid_for(count << c.logn, 256), 256, 0, s>>>(
+        weights, reinterpret_cast<const WeightBlock *>(blocks), out, c.logn, count);
+    return status_from(cudaGetLastError());
+}
+
+}  // namespace tb

@@ -1,0 +1,478 @@
+// MatmulHelper (app/LinearHelper.cuh:197-452) and the continuous-batching
+// MatmulServer over the library's batched device operations.
+#include "serving.hpp"
+
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+namespace troyn {
+
+namespace {
+
+std::size_t ceil_div(std::size_t a, std::size_t b) { return (a + b - 1) / b; }
+
+void cuda_ok(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void tb_ok(int st) {
+    if (st == TB_OK) return;
+    if (st == TB_ERR_INVALID_ARGUMENT) throw std::invalid_argument(tb_last_error());
+    if (st == TB_ERR_UNSUPPORTED) throw std::logic_error(tb_last_error());
+    throw std::runtime_error(tb_last_error());
+}
+
+// uint32 arrays travel packed two per device word.
+DeviceBuffer upload_u32(const std::vector<uint32_t> &v) {
+    std::vector<uint64_t> w((v.size() + 1) / 2, 0);
+    if (!v.empty()) std::memcpy(w.data(), v.data(), v.size() * 4);
+    DeviceBuffer b;
+    b.fromHost(w.data(), w.size());
+    return b;
+}
+
+// Record of tb_matmul_encode_weights: {offset lo, offset hi, in, out, ib, ob, li, lj}.
+void push_block(std::vector<uint32_t> &d, uint64_t src, const MatmulPlan &p, std::size_t bi, std::size_t bj) {
+    d.push_back((uint32_t)src);
+    d.push_back((uint32_t)(src >> 32));
+    d.push_back((uint32_t)p.in);
+    d.push_back((uint32_t)p.out);
+    d.push_back((uint32_t)p.inputBlock);
+    d.push_back((uint32_t)p.outputBlock);
+    d.push_back((uint32_t)(bi * p.inputBlock));
+    d.push_back((uint32_t)(bj * p.outputBlock));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ plan
+
+MatmulPlan MatmulPlan::make(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots) {
+    if (!batch || !in || !out || !slots) throw std::invalid_argument("matmul dimensions must be positive");
+    MatmulPlan p;
+    p.batch = batch;
+    p.in = in;
+    p.out = out;
+    p.slots = slots;
+    std::size_t best = 2147483647;
+    for (std::size_t b = batch; b >= 1; b--) {
+        const std::size_t bc = ceil_div(batch, b);
+        if (b >= slots) continue;
+        if (bc * 2 > best) continue;
+        for (std::size_t i = 1; i < slots / b; i++) {
+            std::size_t o = std::min(slots / b / i, out);
+            if (i > in || o < 1) continue;
+            const std::size_t c = bc * (ceil_div(in, i) + ceil_div(out, o));
+            if (c >= best) continue;
+            p.batchBlock = b;
+            p.inputBlock = i;
+            p.outputBlock = o;
+            best = c;
+        }
+    }
+    if (!p.batchBlock) throw std::invalid_argument("matmul shape does not fit the slot count");
+    return p;
+}
+
+// ------------------------------------------------------------------ helper
+
+Plain2d MatmulHelper::encodeWeights(const BatchEncoder &encoder, const uint64_t *weights) const {
+    const auto &p = plan_;
+    Plain2d out;
+    for (std::size_t li = 0; li < p.in; li += p.inputBlock) {
+        const std::size_t ui = std::min(li + p.inputBlock, p.in);
+        std::vector<Plaintext> row;
+        for (std::size_t lj = 0; lj < p.out; lj += p.outputBlock) {
+            const std::size_t uj = std::min(lj + p.outputBlock, p.out);
+            std::vector<uint64_t> vec(p.inputBlock * p.outputBlock, 0);
+            for (std::size_t j = lj; j < uj; j++)
+                for (std::size_t i = li; i < ui; i++)
+                    vec[(j - lj) * p.inputBlock + p.inputBlock - (i - li) - 1] = weights[i * p.out + j];
+            Plaintext pt;
+            encoder.encodePolynomial(vec, pt);
+            row.push_back(std::move(pt));
+        }
+        out.push_back(std::move(row));
+    }
+    return out;
+}
+
+Plain2d MatmulHelper::encodeInputs(const BatchEncoder &encoder, const uint64_t *inputs) const {
+    const auto &p = plan_;
+    Plain2d out;
+    for (std::size_t li = 0; li < p.batch; li += p.batchBlock) {
+        const std::size_t ui = std::min(li + p.batchBlock, p.batch);
+        std::vector<Plaintext> row;
+        for (std::size_t lj = 0; lj < p.in; lj += p.inputBlock) {
+            const std::size_t uj = std::min(lj + p.inputBlock, p.in);
+            std::vector<uint64_t> vec(p.slots, 0);
+            for (std::size_t i = li; i < ui; i++)
+                for (std::size_t j = lj; j < uj; j++)
+                    vec[(i - li) * p.inputBlock * p.outputBlock + (j - lj)] = inputs[i * p.in + j];
+            Plaintext pt;
+            encoder.encodePolynomial(vec, pt);
+            row.push_back(std::move(pt));
+        }
+        out.push_back(std::move(row));
+    }
+    return out;
+}
+
+Cipher2d MatmulHelper::encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder,
+                                     const uint64_t *inputs) const {
+    Cipher2d out;
+    for (auto &row : encodeInputs(encoder, inputs)) {
+        std::vector<Ciphertext> r;
+        for (auto &pt : row) {
+            Ciphertext c;
+            encryptor.encrypt(pt, c);
+            r.push_back(std::move(c));
+        }
+        out.push_back(std::move(r));
+    }
+    return out;
+}
+
+// MatmulHelper::matmul (app/LinearHelper.cuh:323-346) as one pass: every input
+// transformed once, every weight lifted and transformed once, each output the sum of
+// its products accumulated in one kernel, one inverse transform per output.
+Cipher2d MatmulHelper::matmul(const Evaluator &ev, const Cipher2d &a, const Plain2d &w) const {
+    const auto &p = plan_;
+    const SEALContext &ctx = ev.context();
+    if (ctx.scheme() != SchemeType::bfv && ctx.scheme() != SchemeType::bgv) throw std::logic_error("unsupported scheme");
+    if (a.size() != p.batchBlocks()) throw std::invalid_argument("Input batchsize incorrect.");
+    if (w.size() != p.inputBlocks()) throw std::invalid_argument("Weight input dimension incorrect.");
+    const std::size_t nb = p.batchBlocks(), ni = p.inputBlocks(), no = p.outputBlocks(), n = ctx.polyModulusDegree();
+    const Ciphertext &first = a.at(0).at(0);
+    auto d = ctx.getContextData(first.parmsID());
+    if (!d) throw std::invalid_argument("encrypted is not valid for encryption parameters");
+    const int L = d->levelLimbs();
+    const std::size_t ctw = 2 * (std::size_t)L * n, ptw = (std::size_t)L * n;
+    DeviceBuffer A(nb * ni * ctw), Wr(ni * no * n), Wn(ni * no * ptw), O(nb * no * ctw);
+    for (std::size_t b = 0; b < nb; b++) {
+        if (a[b].size() != ni) throw std::invalid_argument("Input dimension incorrect.");
+        for (std::size_t i = 0; i < ni; i++) {
+            const Ciphertext &c = a[b][i];
+            if (c.parmsID() != first.parmsID() || c.size() != 2 || c.isNttForm() ||
+                c.correctionFactor() != first.correctionFactor())
+                throw std::invalid_argument("inputs must be size-2 ciphertexts of one level and correction factor");
+            cuda_ok(cudaMemcpyAsync(A.get() + (b * ni + i) * ctw, c.data(), ctw * 8, cudaMemcpyDeviceToDevice, 0),
+                    "device copy");
+        }
+    }
+    Wr.zero();
+    for (std::size_t i = 0; i < ni; i++) {
+        if (w[i].size() != no) throw std::invalid_argument("Weight output dimension incorrect.");
+        for (std::size_t j = 0; j < no; j++) {
+            const Plaintext &pt = w[i][j];
+            if (pt.isNttForm() || pt.coeffCount() > n) throw std::invalid_argument("weights must be coefficient plaintexts");
+            if (pt.coeffCount())
+                cuda_ok(cudaMemcpyAsync(Wr.get() + (i * no + j) * n, pt.data(), pt.coeffCount() * 8,
+                                        cudaMemcpyDeviceToDevice, 0),
+                        "device copy");
+        }
+    }
+    std::vector<uint32_t> off{0}, ia, iw;
+    for (std::size_t b = 0; b < nb; b++)
+        for (std::size_t j = 0; j < no; j++) {
+            for (std::size_t i = 0; i < ni; i++) {
+                ia.push_back((uint32_t)(b * ni + i));
+                iw.push_back((uint32_t)(i * no + j));
+            }
+            off.push_back((uint32_t)ia.size());
+        }
+    DeviceBuffer doff = upload_u32(off), dia = upload_u32(ia), diw = upload_u32(iw);
+    tb_context *h = ctx.handle();
+    tb_ok(tb_ntt_forward(h, A.get(), A.get(), 2 * nb * ni, 0, L, 0, nullptr));
+    tb_ok(tb_plain_to_ntt(h, L, Wr.get(), n, n, Wn.get(), ni * no, nullptr));
+    tb_ok(tb_dyadic_accumulate(h, L, 2, A.get(), 0, Wn.get(), 0, O.get(), 0, (const uint32_t *)doff.get(),
+                               (const uint32_t *)dia.get(), (const uint32_t *)diw.get(), (uint32_t)(nb * no), nullptr));
+    tb_ok(tb_ntt_inverse(h, O.get(), O.get(), 2 * nb * no, 0, L, 0, nullptr));
+    Cipher2d out(nb);
+    for (std::size_t b = 0; b < nb; b++)
+        for (std::size_t j = 0; j < no; j++) {
+            Ciphertext c(ctx, first.parmsID(), 2);
+            cuda_ok(cudaMemcpyAsync(c.data(), O.get() + (b * no + j) * ctw, ctw * 8, cudaMemcpyDeviceToDevice, 0),
+                    "device copy");
+            c.correctionFactor() = first.correctionFactor();
+            out[b].push_back(std::move(c));
+        }
+    return out;
+}
+
+std::vector<uint64_t> MatmulHelper::decryptOutputs(const BatchEncoder &encoder, Decryptor &decryptor,
+                                                   const Cipher2d &outputs) const {
+    const auto &p = plan_;
+    std::vector<uint64_t> dec(p.batch * p.out);
+    std::size_t di = 0;
+    for (std::size_t li = 0; li < p.batch; li += p.batchBlock, di++) {
+        const std::size_t ui = std::min(li + p.batchBlock, p.batch);
+        std::size_t dj = 0;
+        for (std::size_t lj = 0; lj < p.out; lj += p.outputBlock, dj++) {
+            const std::size_t uj = std::min(lj + p.outputBlock, p.out);
+            Plaintext pt;
+            decryptor.decrypt(outputs.at(di).at(dj), pt);
+            std::vector<uint64_t> buf;
+            encoder.decodePolynomial(pt, buf);
+            for (std::size_t i = li; i < ui; i++)
+                for (std::size_t j = lj; j < uj; j++)
+                    dec[i * p.out + j] =
+                        buf[(i - li) * p.inputBlock * p.outputBlock + (j - lj) * p.inputBlock + p.inputBlock - 1];
+        }
+    }
+    return dec;
+}
+
+// ------------------------------------------------------------------ server
+
+struct MatmulServer::Wave {
+    std::vector<Request> reqs;
+    std::vector<std::size_t> out_base;   // first output ciphertext of each request
+    std::size_t bytes = 0, out_words = 0;
+    void *dev = nullptr;
+    cudaEvent_t done = nullptr;
+    bool failed = false;
+};
+
+namespace {
+
+std::size_t align256(std::size_t x) { return (x + 255) & ~std::size_t(255); }
+
+}  // namespace
+
+// Pinned staging of one slot, grown on demand (reused only after the slot's previous
+// wave has finished).
+struct MatmulServer::Staging {
+    void *p = nullptr;
+    std::size_t bytes = 0;
+    void ensure(std::size_t need) {
+        if (need <= bytes) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const std::size_t grow = std::max(need, std::size_t(1) << 24);
+        cuda_ok(cudaHostAlloc(&p, grow, cudaHostAllocDefault), "pinned allocation");
+        bytes = grow;
+    }
+    ~Staging() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+namespace {
+}  // namespace
+
+double MatmulServer::now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+MatmulServer::MatmulServer(const SEALContext &context, Options options) : context_(context), opt_(options) {
+    context.requireSet();
+    if (context.scheme() != SchemeType::bfv && context.scheme() != SchemeType::bgv)
+        throw std::logic_error("unsupported scheme");
+    if (opt_.slots < 1 || opt_.slots > 16) throw std::invalid_argument("slots must be in [1, 16]");
+    L_ = context.firstContextData()->levelLimbs();
+    n_ = context.polyModulusDegree();
+    for (int i = 0; i < opt_.slots; i++) {
+        cudaStream_t s;
+        cuda_ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream creation");
+        streams_.push_back(s);
+        pins_.emplace_back(new Staging());  // inputs, weights, records
+        pins_.emplace_back(new Staging());  // outputs
+    }
+}
+
+MatmulServer::~MatmulServer() {
+    for (auto &kv : running_) {
+        cudaEventSynchronize(kv.second->done);
+        cudaEventDestroy(kv.second->done);
+    }
+    for (void *s : streams_) {
+        cudaStreamSynchronize((cudaStream_t)s);
+        cudaStreamDestroy((cudaStream_t)s);
+    }
+}
+
+// Device bytes of one request: inputs, raw and encoded weights, transformed weights,
+// outputs (records and alignment are covered by 64 KiB of slack).
+std::size_t MatmulServer::footprint(const MatmulPlan &p) const {
+    const std::size_t ni = p.inputBlocks(), no = p.outputBlocks(), nw = ni * no;
+    const std::size_t ctw = 2 * (std::size_t)L_ * n_;
+    return 8 * (ni * ctw + p.in * p.out + nw * n_ + nw * (std::size_t)L_ * n_ + no * ctw) + (64u << 10);
+}
+
+uint64_t MatmulServer::submit(std::size_t in, std::size_t out, const uint64_t *inputs, std::size_t input_words,
+                              const uint64_t *weights, double arrival) {
+    MatmulPlan p = MatmulPlan::make(1, in, out, n_);
+    const std::size_t ctw = 2 * (std::size_t)L_ * n_;
+    if (input_words != p.inputBlocks() * ctw) throw std::invalid_argument("input ciphertext words do not match the shape");
+    Request r;
+    r.id = next_id_++;
+    r.in = in;
+    r.out = out;
+    r.plan = p;
+    r.inputs.assign(inputs, inputs + input_words);
+    r.weights.assign(weights, weights + in * out);
+    r.arrival = arrival;
+    r.bytes = footprint(p);
+    if (r.bytes > opt_.memory_budget) throw std::invalid_argument("request larger than the memory budget");
+    queue_.push_back(std::move(r));
+    stats_.submitted++;
+    return queue_.back().id;
+}
+
+bool MatmulServer::launch(int slot) {
+    if (queue_.empty()) return false;
+    auto w = std::make_unique<Wave>();
+    std::size_t bytes = 0;
+    while (!queue_.empty() && w->reqs.size() < opt_.max_wave_requests &&
+           in_flight_bytes_ + bytes + queue_.front().bytes <= opt_.memory_budget) {
+        bytes += queue_.front().bytes;
+        w->reqs.push_back(std::move(queue_.front()));
+        queue_.pop_front();
+    }
+    if (w->reqs.empty()) return false;  // the oldest request waits for memory to free up
+    const std::size_t ctw = 2 * (std::size_t)L_ * n_, ptw = (std::size_t)L_ * n_;
+    // layout: inputs | raw weights | weight records | term offsets | term a | term w  (staged)
+    //         encoded weights | transformed weights | outputs                          (device only)
+    std::size_t na = 0, nw = 0, no = 0, wwords = 0, nterms = 0;
+    std::vector<uint32_t> blocks, off{0}, ia, iw;
+    for (auto &r : w->reqs) {
+        const auto &p = r.plan;
+        const std::size_t ri = p.inputBlocks(), ro = p.outputBlocks();
+        for (std::size_t bi = 0; bi < ri; bi++)
+            for (std::size_t bj = 0; bj < ro; bj++) push_block(blocks, wwords, p, bi, bj);
+        w->out_base.push_back(no);
+        for (std::size_t bj = 0; bj < ro; bj++) {
+            for (std::size_t bi = 0; bi < ri; bi++) {
+                ia.push_back((uint32_t)(na + bi));
+                iw.push_back((uint32_t)(nw + bi * ro + bj));
+            }
+            off.push_back((uint32_t)ia.size());
+        }
+        na += ri;
+        nw += ri * ro;
+        no += ro;
+        wwords += p.in * p.out;
+    }
+    nterms = ia.size();
+    const std::size_t o_in = 0, o_wr = align256(o_in + na * ctw * 8), o_bl = align256(o_wr + wwords * 8),
+                      o_off = align256(o_bl + blocks.size() * 4), o_ia = align256(o_off + off.size() * 4),
+                      o_iw = align256(o_ia + nterms * 4), staged = align256(o_iw + nterms * 4);
+    const std::size_t o_wp = staged, o_wn = align256(o_wp + nw * n_ * 8), o_out = align256(o_wn + nw * ptw * 8),
+                      total = align256(o_out + no * ctw * 8);
+    Staging &pin_in = *pins_[2 * slot], &pin_out = *pins_[2 * slot + 1];
+    pin_in.ensure(staged);
+    pin_out.ensure(no * ctw * 8);
+    char *h = static_cast<char *>(pin_in.p);
+    std::size_t ai = 0, wi = 0;
+    for (auto &r : w->reqs) {
+        std::memcpy(h + o_in + ai * 8, r.inputs.data(), r.inputs.size() * 8);
+        ai += r.inputs.size();
+        std::memcpy(h + o_wr + wi * 8, r.weights.data(), r.weights.size() * 8);
+        wi += r.weights.size();
+    }
+    std::memcpy(h + o_bl, blocks.data(), blocks.size() * 4);
+    std::memcpy(h + o_off, off.data(), off.size() * 4);
+    std::memcpy(h + o_ia, ia.data(), nterms * 4);
+    std::memcpy(h + o_iw, iw.data(), nterms * 4);
+
+    cudaStream_t s = (cudaStream_t)streams_[slot];
+    w->bytes = std::max(bytes, total);
+    w->out_words = no * ctw;
+    cuda_ok(cudaEventCreateWithFlags(&w->done, cudaEventDisableTiming), "event creation");
+    int st = cudaMallocAsync(&w->dev, total, s) == cudaSuccess ? TB_OK : TB_ERR_OUT_OF_MEMORY;
+    char *d = static_cast<char *>(w->dev);
+    auto U = [&](std::size_t o) { return reinterpret_cast<uint64_t *>(d + o); };
+    auto V = [&](std::size_t o) { return reinterpret_cast<const uint32_t *>(d + o); };
+    tb_context *hctx = context_.handle();
+    if (st == TB_OK && cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, s) != cudaSuccess) st = TB_ERR_CUDA;
+    if (st == TB_OK && inject_) st = TB_ERR_CUDA;
+    inject_ = false;
+    if (st == TB_OK) st = tb_ntt_forward(hctx, U(o_in), U(o_in), 2 * na, 0, L_, 0, s);
+    if (st == TB_OK) st = tb_matmul_encode_weights(hctx, U(o_wr), V(o_bl), nw, U(o_wp), s);
+    if (st == TB_OK) st = tb_plain_to_ntt(hctx, L_, U(o_wp), n_, n_, U(o_wn), nw, s);
+    if (st == TB_OK)
+        st = tb_dyadic_accumulate(hctx, L_, 2, U(o_in), 0, U(o_wn), 0, U(o_out), 0, V(o_off), V(o_ia), V(o_iw),
+                                  (uint32_t)no, s);
+    if (st == TB_OK) st = tb_ntt_inverse(hctx, U(o_out), U(o_out), 2 * no, 0, L_, 0, s);
+    if (st == TB_OK && cudaMemcpyAsync(pin_out.p, U(o_out), no * ctw * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        st = TB_ERR_CUDA;
+    w->failed = st != TB_OK;
+    if (w->dev) cudaFreeAsync(w->dev, s);
+    cuda_ok(cudaEventRecord(w->done, s), "event record");
+    in_flight_bytes_ += w->bytes;
+    stats_.waves++;
+    stats_.max_wave = std::max(stats_.max_wave, w->reqs.size());
+    stats_.peak_bytes = std::max(stats_.peak_bytes, in_flight_bytes_);
+    running_[slot] = std::move(w);
+    return true;
+}
+
+void MatmulServer::reap(std::vector<uint64_t> &finished) {
+    for (auto it = running_.begin(); it != running_.end();) {
+        Wave &w = *it->second;
+        const cudaError_t q = cudaEventQuery(w.done);
+        if (q == cudaErrorNotReady) {
+            ++it;
+            continue;
+        }
+        const bool ok = q == cudaSuccess && !w.failed;
+        const double t = now();
+        const uint64_t *out = static_cast<const uint64_t *>(pins_[2 * it->first + 1]->p);
+        const std::size_t ctw = 2 * (std::size_t)L_ * n_;
+        for (std::size_t k = 0; k < w.reqs.size(); k++) {
+            const Request &r = w.reqs[k];
+            Done d;
+            d.arrival = r.arrival;
+            d.done = t;
+            d.ok = ok;
+            if (ok) {
+                const std::size_t words = r.plan.outputBlocks() * ctw;
+                d.outputs.assign(out + w.out_base[k] * ctw, out + w.out_base[k] * ctw + words);
+            }
+            done_[r.id] = std::move(d);
+            finished.push_back(r.id);
+            if (ok)
+                stats_.completed++;
+            else
+                stats_.failed++;
+        }
+        in_flight_bytes_ -= w.bytes;
+        cudaEventDestroy(w.done);
+        it = running_.erase(it);
+    }
+}
+
+std::vector<uint64_t> MatmulServer::step() {
+    std::vector<uint64_t> finished;
+    reap(finished);
+    for (int slot = 0; slot < opt_.slots && !queue_.empty(); slot++)
+        if (!running_.count(slot)) launch(slot);
+    return finished;
+}
+
+bool MatmulServer::drain(double timeout) {
+    const double end = now() + timeout;
+    while (!idle()) {
+        step();
+        if (now() > end) return false;
+    }
+    return true;
+}
+
+bool MatmulServer::result(uint64_t id, std::vector<uint64_t> &outputs, double &arrival, double &done, bool &ok) {
+    auto it = done_.find(id);
+    if (it == done_.end()) return false;
+    outputs = it->second.outputs;
+    arrival = it->second.arrival;
+    done = it->second.done;
+    ok = it->second.ok;
+    return true;
+}
+
+}  // namespace troyn

@@ -1,0 +1,141 @@
+// Encrypted vector x plaintext-matrix products (the reference's app/LinearHelper.cuh
+// MatmulHelper, coefficient encoding) and a continuous-batching server for them.
+//
+// MatmulHelper keeps the reference's block planning and encodings; its matmul runs
+// every product of a call in one pass on the device (inputs transformed once,
+// weights lifted and transformed once, all sums of products accumulated in one
+// kernel, one inverse transform per output) instead of one multiplyPlain and
+// addInplace per block pair. The sums are exact, so outputs are word-identical.
+//
+// MatmulServer serves a stream of single-row requests of different shapes: requests
+// wait in a FIFO queue; whenever one of its `slots` streams is free it admits queued
+// requests (oldest first) while their device footprint fits the memory budget, and
+// runs them together as one wave (one set of launches over all admitted requests) on
+// that stream. Waves on different streams overlap on the device. Each request's
+// arithmetic depends only on its own data, so a result is the same whether the
+// request ran alone or in a mix.
+#pragma once
+
+#include <chrono>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "troy_b200.hpp"
+
+namespace troyn {
+
+// Block shape of MatmulHelper::determineBlock (app/LinearHelper.cuh:206-228).
+struct MatmulPlan {
+    std::size_t batch = 0, in = 0, out = 0, slots = 0;
+    std::size_t batchBlock = 0, inputBlock = 0, outputBlock = 0;
+    static MatmulPlan make(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots);
+    std::size_t batchBlocks() const { return (batch + batchBlock - 1) / batchBlock; }
+    std::size_t inputBlocks() const { return (in + inputBlock - 1) / inputBlock; }
+    std::size_t outputBlocks() const { return (out + outputBlock - 1) / outputBlock; }
+};
+
+using Plain2d = std::vector<std::vector<Plaintext>>;
+using Cipher2d = std::vector<std::vector<Ciphertext>>;
+
+class MatmulHelper {
+public:
+    MatmulHelper(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots)
+        : plan_(MatmulPlan::make(batch, in, out, slots)) {}
+    const MatmulPlan &plan() const { return plan_; }
+    // encodeWeights / encodeInputs / encryptInputs / decryptOutputs
+    // (app/LinearHelper.cuh:258-452): coefficient encodings of the reference.
+    Plain2d encodeWeights(const BatchEncoder &encoder, const std::uint64_t *weights) const;
+    Plain2d encodeInputs(const BatchEncoder &encoder, const std::uint64_t *inputs) const;
+    Cipher2d encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder, const std::uint64_t *inputs) const;
+    Cipher2d matmul(const Evaluator &evaluator, const Cipher2d &a, const Plain2d &w) const;
+    std::vector<std::uint64_t> decryptOutputs(const BatchEncoder &encoder, Decryptor &decryptor,
+                                              const Cipher2d &outputs) const;
+
+private:
+    MatmulPlan plan_;
+};
+
+class MatmulServer {
+public:
+    struct Options {
+        std::size_t memory_budget = std::size_t(8) << 30;  // device bytes of admitted requests
+        int slots = 3;                                     // waves in flight (one stream each)
+        std::size_t max_wave_requests = 256;
+    };
+    struct Stats {
+        std::uint64_t submitted = 0, completed = 0, failed = 0, waves = 0;
+        std::size_t peak_bytes = 0, max_wave = 0;
+    };
+
+    MatmulServer(const SEALContext &context, Options options);
+    ~MatmulServer();
+    MatmulServer(const MatmulServer &) = delete;
+    MatmulServer &operator=(const MatmulServer &) = delete;
+
+    // Seconds on the steady clock the server stamps completions with.
+    static double now();
+
+    // Queues one request: `inputs` are the encrypted input ciphertexts at the first
+    // level, in order (plan.inputBlocks() ciphertexts of 2 x L x N words),
+    // `weights` the row-major in x out matrix mod t. arrival is a now() stamp.
+    // Returns the request id; throws std::invalid_argument on inconsistent sizes or a
+    // request larger than the whole memory budget.
+    std::uint64_t submit(std::size_t in, std::size_t out, const std::uint64_t *inputs, std::size_t input_words,
+                         const std::uint64_t *weights, double arrival);
+    // Non-blocking: collects finished waves, then launches new waves on free slots.
+    // Returns the ids that finished during this call.
+    std::vector<std::uint64_t> step();
+    // Steps until every queued and running request has finished or `timeout` seconds
+    // passed; returns false on timeout.
+    bool drain(double timeout);
+    bool idle() const { return queue_.empty() && running_.empty(); }
+    std::size_t queued() const { return queue_.size(); }
+    // Output ciphertexts (plan.outputBlocks() x 2 x L x N words) of a finished request,
+    // with its arrival and completion stamps; false if unknown or not finished.
+    // `ok` is false for a request whose wave failed.
+    bool result(std::uint64_t id, std::vector<std::uint64_t> &outputs, double &arrival, double &done, bool &ok);
+    void release(std::uint64_t id) { done_.erase(id); }
+    const Stats &stats() const { return stats_; }
+    // Makes the next launched wave report a failed library call (a host-side fault
+    // injection for tests of the failure path; no device work is altered).
+    void injectWaveFailure() { inject_ = true; }
+
+private:
+    struct Request {
+        std::uint64_t id;
+        std::size_t in, out;
+        MatmulPlan plan;
+        std::vector<std::uint64_t> inputs, weights;
+        double arrival;
+        std::size_t bytes;
+    };
+    struct Wave;
+    struct Staging;
+    struct Done {
+        std::vector<std::uint64_t> outputs;
+        double arrival, done;
+        bool ok;
+    };
+    std::size_t footprint(const MatmulPlan &p) const;
+    bool launch(int slot);
+    void reap(std::vector<std::uint64_t> &finished);
+
+    const SEALContext &context_;
+    Options opt_;
+    int L_ = 0;
+    std::size_t n_ = 0;
+    std::uint64_t next_id_ = 1;
+    std::size_t in_flight_bytes_ = 0;
+    bool inject_ = false;
+    std::deque<Request> queue_;
+    std::vector<void *> streams_;
+    std::vector<std::unique_ptr<Staging>> pins_;  // per slot: staged inputs, outputs
+    std::map<int, std::unique_ptr<Wave>> running_;
+    std::map<std::uint64_t, Done> done_;
+    Stats stats_;
+};
+
+}  // namespace troyn

@@ -1157,16 +1157,23 @@ void BatchEncoder::decode(const Plaintext &plain, std::vector<int64_t> &dest) co
         dest[i] = u[i] > (t >> 1) ? (int64_t)u[i] - (int64_t)t : (int64_t)u[i];
 }
 
+// BatchEncoderCuda::encodePolynomial (src/batchencoder_cuda.cu:124-144): the values,
+// each reduced mod t, as coefficients.
 void BatchEncoder::encodePolynomial(const std::vector<uint64_t> &values, Plaintext &dest) const {
     if (values.size() > slots_) throw std::invalid_argument("values_matrix size is too large");
+    const uint64_t t = context_.firstContextData()->parms().plainModulus().value();
+    std::vector<uint64_t> v(values.size());
+    for (std::size_t i = 0; i < v.size(); i++) v[i] = values[i] % t;
     Plaintext p;
-    p.fromHost(values);
+    p.fromHost(v);
     dest = std::move(p);
 }
 
+// BatchEncoderCuda::decodePolynomial (src/batchencoder_cuda.cu:267-270): N coefficients.
 void BatchEncoder::decodePolynomial(const Plaintext &plain, std::vector<uint64_t> &dest) const {
     if (plain.isNttForm()) throw std::invalid_argument("plain cannot be in NTT form");
     dest = plain.toHost();
+    dest.resize(slots_, 0);
 }
 
 CKKSEncoder::CKKSEncoder(const SEALContext &context) : context_(context), slots_(context.polyModulusDegree() / 2) {
