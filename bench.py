@@ -17,6 +17,11 @@ prime (the arithmetic performed is the same as on encrypted data).
 * ``roofline``: the dominant kernel from the library's per-launch event trace.
 * ``cpu_baseline``: the reference's own CPU implementation (compiled under
   oracle/_ref) on a bounded sample of the same workload, one process per core.
+* ``plain_per_op``: the same chain driven one pair per call (batch 1), as the
+  reference's evaluator is used; ``batched_over_per_op`` is the batching gain.
+* ``serving``: the serving loop (MatmulServer, BFV N = 8192, 5 primes): Poisson
+  arrivals of encrypted vector x matrix requests at several rates plus a burst,
+  p50/p99 latency and throughput per rate.
 
 ``--impl reference`` times only that CPU implementation as the benchmark line.
 With ``--gpus N`` (torchrun, one rank per GPU) every rank runs an independent
@@ -31,7 +36,6 @@ import math
 import multiprocessing as mp
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -48,6 +52,12 @@ STEPS_K = [1 << i for i in range(13)]
 METRIC = "HE mul+relin+rescale+rotate ops/s (CKKS N=16384, batched 64 pairs)"
 WORKLOAD = "ckks_n16384_L8_batch64_mul_relin_rescale_rotate"
 FALLBACK_HBM_GBS = 6650.0
+PER_OP_PAIRS = 16
+# serving workload: encrypted vector x plaintext matrix (MatmulHelper coefficient
+# encoding), BFV N = 8192, 5 primes, 20-bit batching t, Poisson arrivals
+SERVE_N = 8192
+SERVE_BITS = [43, 43, 44, 44, 44]
+SERVE_RATES = [10, 200, 1000, 2000]
 
 
 def _peak_hbm():
@@ -61,58 +71,60 @@ def _peak_hbm():
 
 # ------------------------------------------------------------ clocks sampler
 class ClockSampler:
-    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons of the benchmark's
+    GPU every 5 ms through NVML while the timed region runs, so that even a region
+    of a few tens of milliseconds gets samples; falls back to nvidia-smi."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, device):
+        self.device = device
+        self.samples, self.mask, self.max_mhz = [], 0, None
+        self.stop_flag = threading.Event()
+        self.t = None
+        self.err = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _run(self):
+        try:
+            import pynvml
+            h = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            while not self.stop_flag.is_set():
+                self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                self.mask |= int(reasons(h))
+                time.sleep(0.005)
+        except Exception as e:  # NVML missing or refused: report it
+            self.err = f"{type(e).__name__}: {e}"
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        time.sleep(0.02)
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        self.stop_flag.set()
+        if self.t:
+            self.t.join(timeout=5)
+        if self.err or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [self.err or "no samples"], "samples": 0}
+        reasons = sorted(k for k, bit in self.REASONS.items() if self.mask & bit)
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "NVML every 5 ms"}
 
 
-# ------------------------------------------------------------------ B200 arm
 def _rand_residues(torch, shape, moduli, gen):
     """uint64 residues (stored as int64) uniform modulo moduli[l] along axis -2 (two launches)."""
     # q < 2^61: 62 random bits reduced mod q (negligible bias for a benchmark input)
@@ -201,6 +213,27 @@ def run_b200(args, rank, world):
     trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms)) for i in range(cnt.value)}
     launches = sum(v[0] for v in trace.values()) // args.steps
 
+    # plain per-op form: one ciphertext pair per call chain (batch 1), the way the
+    # reference evaluator is driven (one multiply / relinearize / rescale / rotate call
+    # per ciphertext); same kernels, same keys
+    def per_op_chain(i):
+        g = i % len(STEPS_K)
+        ctx("multiply", L, A[i:i + 1], 0, B[i:i + 1], 0, T3[0:1], 0, 1, stream)
+        ctx("relinearize", L, T3[0:1], 0, rlk, 1, stream)
+        ctx("rescale_to_next", L, T3[0:1], 3 * L * N, R[0:1], 0, 2, 1, stream)
+        ctx("apply_galois", L - 1, elts[g], R[0:1], 0, O[i:i + 1], 0, gks[g], 1, stream)
+
+    per_op_pairs = min(PAIRS, PER_OP_PAIRS)
+    for i in range(2):
+        per_op_chain(i)
+    barrier()
+    e0.record(stream)
+    for i in range(per_op_pairs):
+        per_op_chain(i)
+    e1.record(stream)
+    barrier()
+    per_op_ms = e0.elapsed_time(e1) / per_op_pairs
+
     # end to end through the C ABI with host buffers
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
@@ -227,11 +260,94 @@ def run_b200(args, rank, world):
 
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        t = torch.tensor([ms, e2e_ms, per_op_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    return {"ms": ms, "e2e_ms": e2e_ms, "trace": trace, "launches": launches, "clocks": clk,
+        ms, e2e_ms, per_op_ms = float(t[0]), float(t[1]), float(t[2])
+    return {"ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
+
+
+def _pinned(a):
+    """A page-locked copy of a uint64 array (what a server's receive buffers would be)."""
+    import numpy as np
+    import torch
+    t = torch.empty(a.size, dtype=torch.int64, pin_memory=True)
+    out = t.numpy().view(np.uint64)
+    out[:] = a
+    _pinned.keep.append(t)
+    return out
+
+
+_pinned.keep = []
+
+
+def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
+    """Poisson arrivals of encrypted vector x matrix requests (input dimension in
+    {64, ..., 1024}, output in {16, ..., 256}, seeded) through MatmulServer at each rate
+    of SERVE_RATES plus one burst with every request queued at once. Latency is
+    arrival to completion on the host steady clock; throughput is completed requests
+    over first arrival to last completion."""
+    sys.path.insert(0, os.path.join(ROOT, "seal-cuda_b200", "lib"))
+    import numpy as np
+    import pytroy
+
+    t = pytroy.PlainModulus.batching(SERVE_N, 20)
+    p = pytroy.EncryptionParameters(pytroy.SchemeType.bfv)
+    p.set_poly_modulus_degree(SERVE_N)
+    p.set_coeff_modulus(pytroy.CoeffModulus.create(SERVE_N, SERVE_BITS))
+    p.set_plain_modulus(t)
+    ctx = pytroy.SEALContext(p)
+    keygen = pytroy.KeyGenerator(ctx)
+    enc = pytroy.BatchEncoder(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    rng = np.random.default_rng(2718)
+    pool = []
+    for _ in range(pool_size):
+        inp, out = int(rng.integers(1, 17)) * 64, int(rng.integers(1, 17)) * 16
+        x = rng.integers(0, t.value(), inp, dtype=np.uint64)
+        w = rng.integers(0, t.value(), inp * out, dtype=np.uint64)
+        h = pytroy.MatmulHelper(1, inp, out, SERVE_N)
+        cts = h.encrypt_inputs(encryptor, enc, x)
+        words = np.concatenate([np.asarray(c.data(), np.uint64) for c in cts[0]])
+        pool.append((inp, out, _pinned(words), _pinned(w)))
+    server = pytroy.MatmulServer(ctx, memory_budget=16 << 30, slots=3)
+    now = pytroy.MatmulServer.now
+    for r in pool[:8]:  # warm-up
+        server.submit(r[0], r[1], r[2], r[3], now())
+    server.drain(60.0)
+
+    def run(rate):
+        count = max_requests if rate is None else max(20, min(max_requests, int(rate * seconds_per_rate)))
+        gaps = np.zeros(count) if rate is None else rng.exponential(1.0 / rate, count)
+        start = now()
+        due = start + np.cumsum(gaps)
+        ids, k = [], 0
+        waves0 = server.stats()["waves"]
+        while k < count or not server.idle():
+            tnow = now()
+            while k < count and due[k] <= tnow:
+                r = pool[k % len(pool)]
+                ids.append(server.submit(r[0], r[1], r[2], r[3], float(due[k])))
+                k += 1
+            server.step()
+            if tnow - start > 120.0:
+                raise RuntimeError("serving run did not finish")
+        lat, first, last, ok = [], None, None, 0
+        for rid in ids:
+            _, arrival, done, good = server.take(rid)
+            ok += bool(good)
+            lat.append(1e3 * (done - arrival))
+            first = arrival if first is None else min(first, arrival)
+            last = done if last is None else max(last, done)
+        waves = server.stats()["waves"] - waves0
+        return {"rate_rps": rate if rate is not None else "burst", "requests": count, "ok": ok,
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "throughput_rps": round(count / (last - first), 1), "mean_wave": round(count / max(1, waves), 2)}
+
+    runs = [run(r) for r in SERVE_RATES] + [run(None)]
+    return {"workload": "bfv_n8192_L4_matmul_poisson", "slots": 3, "memory_budget_gb": 16,
+            "request_shapes": "in {64..1024} x out {16..256}, MatmulHelper coefficient encoding",
+            "latency": "arrival to completion, host steady clock", "runs": runs}
 
 
 class tb_capi_trace_entry(ctypes.Structure):
@@ -367,6 +483,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker in the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
                     help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
@@ -416,6 +533,8 @@ def main():
             v, ops, busy, wall = cpu_reference(args.cpu_ops, workers)
             cpu = {"value": round(v, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
                    "sample": f"{ops} ops ({args.cpu_ops} per process x {workers} processes), {busy:.1f} s"}
+        per_op = 1e3 / res["per_op_ms"]
+        serving = None if args.no_serving else run_serving()
         line = {"metric": METRIC, "value": round(value, 2), "unit": "ops/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(res["ms"], 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact modular)",
@@ -428,6 +547,10 @@ def main():
                 "gpu_launches": res["launches"],
                 "roofline": roofline(res, args.steps),
                 "cpu_baseline": cpu,
+                "plain_per_op": {"value": round(per_op * world, 2), "unit": "ops/s", "pairs": res["per_op_pairs"],
+                                 "form": "one pair per call chain (batch 1), same kernels and keys",
+                                 "batched_over_per_op": round(value / (per_op * world), 2)},
+                "serving": serving,
                 "clocks": res["clocks"],
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(res["trace"].items())}}
         print(json.dumps(line))

@@ -529,20 +529,26 @@ PYBIND11_MODULE(pytroy, m) {
 
     // Continuous-batching server of single-row MatmulHelper products.
     py::class_<MatmulServer>(m, "MatmulServer")
-        .def(py::init([](const SEALContext &ctx, std::size_t memory_budget, int slots, std::size_t max_wave_requests) {
+        .def(py::init([](const SEALContext &ctx, std::size_t memory_budget, int slots, std::size_t max_wave_requests,
+                         std::size_t output_staging) {
                  MatmulServer::Options o;
                  o.memory_budget = memory_budget;
                  o.slots = slots;
                  o.max_wave_requests = max_wave_requests;
+                 o.output_staging = output_staging;
                  return std::make_unique<MatmulServer>(ctx, o);
              }),
              py::arg("context"), py::arg("memory_budget") = std::size_t(8) << 30, py::arg("slots") = 3,
-             py::arg("max_wave_requests") = 256, py::keep_alive<1, 2>())
+             py::arg("max_wave_requests") = 256, py::arg("output_staging") = std::size_t(256) << 20,
+             py::keep_alive<1, 2>())
         .def_static("now", &MatmulServer::now)
         .def("submit",
              [](MatmulServer &s, std::size_t in, std::size_t out, U64Array inputs, U64Array weights, double arrival) {
                  if ((std::size_t)weights.size() != in * out) throw std::invalid_argument("Weight size incorrect.");
-                 return s.submit(in, out, inputs.data(), inputs.size(), weights.data(), arrival);
+                 // the arrays are read at admission; holding them here keeps them alive
+                 // (requests are admitted and released inside step(), with the GIL held)
+                 auto owner = std::make_shared<std::pair<U64Array, U64Array>>(inputs, weights);
+                 return s.submitBorrowed(in, out, inputs.data(), inputs.size(), weights.data(), arrival, owner);
              })
         .def("step", &MatmulServer::step)
         .def("drain", &MatmulServer::drain)
@@ -556,6 +562,19 @@ PYBIND11_MODULE(pytroy, m) {
                  if (!s.result(id, out, arrival, done, ok)) return py::none();
                  return py::make_tuple(to_array(out), arrival, done, ok);
              })
+        .def("take",
+             [](MatmulServer &s, std::uint64_t id) -> py::object {
+                 auto *out = new vector<uint64_t>();
+                 double arrival = 0, done = 0;
+                 bool ok = false;
+                 if (!s.take(id, *out, arrival, done, ok)) {
+                     delete out;
+                     return py::none();
+                 }
+                 py::capsule owner(out, [](void *p) { delete static_cast<vector<uint64_t> *>(p); });
+                 py::array_t<uint64_t> arr({(py::ssize_t)out->size()}, {(py::ssize_t)8}, out->data(), owner);
+                 return py::make_tuple(arr, arrival, done, ok);
+             })
         .def("release", &MatmulServer::release)
         .def("inject_wave_failure", &MatmulServer::injectWaveFailure)
         .def("stats", [](const MatmulServer &s) {
@@ -567,6 +586,9 @@ PYBIND11_MODULE(pytroy, m) {
             d["waves"] = st.waves;
             d["peak_bytes"] = st.peak_bytes;
             d["max_wave"] = st.max_wave;
+            d["launch_host_s"] = st.launch_host_s;
+            d["reap_host_s"] = st.reap_host_s;
+            d["device_s"] = st.device_s;
             return d;
         });
 }

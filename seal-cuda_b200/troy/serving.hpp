@@ -64,10 +64,13 @@ public:
         std::size_t memory_budget = std::size_t(8) << 30;  // device bytes of admitted requests
         int slots = 3;                                     // waves in flight (one stream each)
         std::size_t max_wave_requests = 256;
+        std::size_t output_staging = std::size_t(256) << 20;  // page-locked result bytes per slot
     };
     struct Stats {
         std::uint64_t submitted = 0, completed = 0, failed = 0, waves = 0;
         std::size_t peak_bytes = 0, max_wave = 0;
+        double launch_host_s = 0, reap_host_s = 0;  // host time inside launch / reap
+        double device_s = 0;                        // sum of wave durations on the device
     };
 
     MatmulServer(const SEALContext &context, Options options);
@@ -85,6 +88,13 @@ public:
     // request larger than the whole memory budget.
     std::uint64_t submit(std::size_t in, std::size_t out, const std::uint64_t *inputs, std::size_t input_words,
                          const std::uint64_t *weights, double arrival);
+    // The same without copying at submission: `inputs` and `weights` are read when the
+    // request is admitted, and `owner` (may be null) is held until they have been read;
+    // the caller keeps the memory unchanged meanwhile. Page-locked (pinned) memory is
+    // copied to the device directly; other memory goes through the slot's staging.
+    std::uint64_t submitBorrowed(std::size_t in, std::size_t out, const std::uint64_t *inputs,
+                                 std::size_t input_words, const std::uint64_t *weights, double arrival,
+                                 std::shared_ptr<void> owner);
     // Non-blocking: collects finished waves, then launches new waves on free slots.
     // Returns the ids that finished during this call.
     std::vector<std::uint64_t> step();
@@ -97,6 +107,8 @@ public:
     // with its arrival and completion stamps; false if unknown or not finished.
     // `ok` is false for a request whose wave failed.
     bool result(std::uint64_t id, std::vector<std::uint64_t> &outputs, double &arrival, double &done, bool &ok);
+    // result() that hands the outputs over without a copy and forgets the request.
+    bool take(std::uint64_t id, std::vector<std::uint64_t> &outputs, double &arrival, double &done, bool &ok);
     void release(std::uint64_t id) { done_.erase(id); }
     const Stats &stats() const { return stats_; }
     // Makes the next launched wave report a failed library call (a host-side fault
@@ -108,7 +120,9 @@ private:
         std::uint64_t id;
         std::size_t in, out;
         MatmulPlan plan;
-        std::vector<std::uint64_t> inputs, weights;
+        const std::uint64_t *in_ptr = nullptr, *w_ptr = nullptr;
+        std::shared_ptr<void> owner;                  // keeps borrowed memory alive
+        bool pinned = false;                          // both arrays page-locked: direct copies
         double arrival;
         std::size_t bytes;
     };

@@ -307,6 +307,14 @@ SEALContext::SEALContext(EncryptionParameters parms, bool expand_mod_chain, Secu
     const int sch = scheme_ == SchemeType::bfv ? TB_SCHEME_BFV : (scheme_ == SchemeType::bgv ? TB_SCHEME_BGV : TB_SCHEME_CKKS);
     check(tb_context_create(sch, n_, qv.data(), K_, parms.plainModulus().value(), &h));
     handle_ = std::shared_ptr<tb_context>(h, [](tb_context *p) { tb_context_destroy(p); });
+    // containers allocate from the device's stream-ordered pool: keep freed blocks for
+    // reuse instead of returning them to the driver at every synchronisation
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
 }
 
 void SEALContext::requireSet() const {
