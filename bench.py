@@ -190,6 +190,11 @@ def run_b200(args, rank, world):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # the autotuner times this step under each setting of the library's speed knobs
+    # (NTT launch variants, key-switch budget; all compute identical words) and keeps
+    # the fastest
+    import tuning
+    tuned = tuning.tune_step(lambda: step(A, B, O), 14, stream)
     for _ in range(args.warmup):
         step(A, B, O)
     barrier()
@@ -263,7 +268,8 @@ def run_b200(args, rank, world):
         t = torch.tensor([ms, e2e_ms, per_op_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_ms, per_op_ms = float(t[0]), float(t[1]), float(t[2])
-    return {"ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
+    return {"tuned": tuned,
+            "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
 
 
@@ -541,7 +547,7 @@ def main():
                 "data": "synthetic: seeded uniform residues for ciphertexts and keys",
                 "config": {"workload": WORKLOAD, "global_batch": ops_total, "seq_len": N,
                            "parallelism": "replicas" if world > 1 else "single GPU",
-                           "l2": "inputs (256 MB) larger than L2"},
+                           "l2": "inputs (256 MB) larger than L2", "tuned": res["tuned"]},
                 "e2e": {"value": round(e2e, 2), "unit": "ops/s", "h2d_bytes_per_step": res["h2d"],
                         "d2h_bytes_per_step": res["d2h"]},
                 "gpu_launches": res["launches"],

@@ -346,6 +346,25 @@ int tb_sub(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_strid
 int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_stride, uint64_t *out,
               uint64_t out_stride, uint64_t batch, void *stream);
 
+/* ---------------------------------------------------------------- tuning
+ *
+ * Speed knobs; every setting computes the same words. No counterpart in the reference
+ * (its kernels have fixed launch shapes). Settings are process-wide.
+ */
+
+/* NTT launch variant for one direction and log2 block size (12..14 have variants 0
+   and 1: the default thread count, and half of it with two radix-8 groups per thread). */
+int tb_ntt_set_variant(int forward, int log_block, int variant);
+int tb_ntt_get_variant(int forward, int log_block, int *variant);
+/* Times both variants of the context's transform size on `polys` scratch limbs (0 =
+   256) with CUDA events on `stream` and keeps the faster per direction. */
+int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_variant, int *inverse_variant);
+/* Scratch budget of one key-switch launch sequence: a batch whose intermediates exceed
+   it is processed in chunks (default 2 GiB, or the TB_KS_SCRATCH_BYTES environment
+   value; 0 restores the default). */
+int tb_keyswitch_set_budget(uint64_t bytes);
+uint64_t tb_keyswitch_get_budget(void);
+
 /* ---------------------------------------------------------------- tracing */
 
 /* Per-kernel device time of the library's launches (CUDA events on each launch's

@@ -64,6 +64,7 @@ int ckks_decode_polynomial(Context &c, int L, const uint64_t *plain, double scal
                            uint64_t B, cudaStream_t s);
 int ckks_encode_double(Context &c, int L, double value, double scale, uint64_t *out, cudaStream_t s);
 int ckks_encode_int64(Context &c, int L, int64_t value, uint64_t *out, cudaStream_t s);
+int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, int *chosen_inv);
 int matmul_encode_weights(Context &c, const uint64_t *weights, const uint32_t *blocks, uint64_t count, uint64_t *out,
                           cudaStream_t s);
 int dyadic_accumulate(const Context &c, int L, int size, const uint64_t *a, uint64_t astride, const uint64_t *w,
@@ -363,6 +364,12 @@ int tb_matmul_encode_weights(tb_context *ctx, const uint64_t *weights, const uin
                              uint64_t *plain, void *stream) {
     return on_device(ctx, [&](tb::Context &c) {
         return tb::matmul_encode_weights(c, weights, blocks, count, plain, S(stream));
+    });
+}
+
+int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_variant, int *inverse_variant) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::autotune_ntt(c, polys, S(stream), forward_variant, inverse_variant);
     });
 }
 

@@ -24,6 +24,7 @@
 #include "trace.cuh"
 
 namespace tb {
+size_t ks_scratch_budget();
 
 unsigned grid_for(uint64_t work, int threads);
 
@@ -344,10 +345,7 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
     const size_t per_ct = ((ckks ? (size_t)L : 0) + (size_t)L * (L + 1) + 2ull * (L + 1) + 2) * n * 8;
     // Whole batches per launch keep every stage's grid several waves deep; the batch is
     // only split when its intermediates would exceed the scratch budget.
-    static const size_t budget = [] {
-        const char *v = getenv("TB_KS_SCRATCH_BYTES");
-        return v ? (size_t)strtoull(v, nullptr, 10) : (size_t)(2ull << 30);
-    }();
+    const size_t budget = ks_scratch_budget();
     uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(B, budget / per_ct));
     ensure_pool_retains(c.device);
     Scratch scr(s);

@@ -33,10 +33,15 @@ struct NttLimb {
     uint32_t sb;                 // sub-block index when the CTA owns 2^LOGB of a longer limb
 };
 
-template <int LOGB>
+// Threads per CTA: variant 0 gives each thread one radix-8 group per pass at a time (at
+// most 1024 threads); variant V >= 1 divides the thread count by 2^V, each thread then
+// running its groups of a pass side by side (more independent work per thread, more
+// registers per thread). The variant per block size is a tuning choice (tb_ntt_*).
+template <int LOGB, int V = 0>
 struct NttCfg {
     static constexpr int NB = 1 << LOGB;
-    static constexpr int THREADS = NB >= 8192 ? 1024 : (NB / 8 >= 64 ? NB / 8 : 64);
+    static constexpr int BASE = NB >= 8192 ? 1024 : (NB / 8 >= 64 ? NB / 8 : 64);
+    static constexpr int THREADS = (BASE >> V) >= 32 ? (BASE >> V) : 32;
     static constexpr int REM = LOGB % 3;
 };
 
@@ -57,59 +62,83 @@ __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong
 // ---------------------------------------------------------------- forward
 // Pass of R_LOG Cooley-Tukey stages starting at local stage s. rbase = 2^s0 + sb
 // where s0 is the global stage of local stage 0 (0 when the CTA owns the limb).
-template <int R_LOG, bool FROM_GLOBAL, int LOGB, class Op, class Ctx>
-__device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *sm, int s, uint32_t rbase) {
+// SIDE: the thread's groups are processed side by side (all loaded, then all
+// butterflies, then all stored: more independent work, more registers) rather than
+// one after another.
+template <int R_LOG, bool FROM_GLOBAL, int LOGB, int T, int s, bool SIDE, class Op, class Ctx>
+__device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     constexpr int R = 1 << R_LOG;
     constexpr int NB = 1 << LOGB;
     constexpr int G = NB >> R_LOG;
-    constexpr int T = NttCfg<LOGB>::THREADS;
+    constexpr int IT = G > 0 ? (G + T - 1) / T : 1;  // groups per thread
+    constexpr int GR = SIDE ? IT : 1;                // groups in flight at once
+    constexpr bool FULL = G > 0 && G % T == 0;
+    constexpr int logsub = LOGB - s - R_LOG;
     const uint64_t q = c.lm.q, q2 = q << 1;
-    const int logsub = LOGB - s - R_LOG;
-    for (int g = threadIdx.x; g < G; g += T) {
-        const int j = g & ((1 << logsub) - 1);
-        const int bi = g >> logsub;
-        const int base = (bi << (LOGB - s)) + j;
-        uint64_t v[R];
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-            const int e = base + (k << logsub);
-            if constexpr (FROM_GLOBAL) v[k] = op.load(c, e);
-            else v[k] = sm[swz(e)];
-        }
-        const uint32_t X = (rbase << s) + (uint32_t)bi;
+    for (int i0 = 0; i0 < IT; i0 += GR) {
+        uint64_t v[GR][R];
 #pragma unroll
-        for (int t = 0; t < R_LOG; t++) {
-            const int half = R >> (t + 1);
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const int base = ((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1));
 #pragma unroll
             for (int k = 0; k < R; k++) {
-                if (k & half) continue;
-                const uint32_t ri = (X << t) + (uint32_t)(k >> (R_LOG - t));
-                ct_butterfly(v[k], v[k + half], __ldg(&c.lm.roots[ri]), q, q2);
+                const int e = base + (k << logsub);
+                if constexpr (FROM_GLOBAL) v[it][k] = op.load(c, e);
+                else v[it][k] = sm[swz(e)];
             }
         }
 #pragma unroll
-        for (int k = 0; k < R; k++) sm[swz(base + (k << logsub))] = v[k];
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const uint32_t X = (rbase << s) + (uint32_t)(g >> logsub);
+#pragma unroll
+            for (int t = 0; t < R_LOG; t++) {
+                const int half = R >> (t + 1);
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    if (k & half) continue;
+                    const uint32_t ri = (X << t) + (uint32_t)(k >> (R_LOG - t));
+                    ct_butterfly(v[it][k], v[it][k + half], __ldg(&c.lm.roots[ri]), q, q2);
+                }
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const int base = ((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1));
+#pragma unroll
+            for (int k = 0; k < R; k++) sm[swz(base + (k << logsub))] = v[it][k];
+        }
     }
     __syncthreads();
 }
 
-template <int LOGB, class Op>
-__global__ void __launch_bounds__(NttCfg<LOGB>::THREADS) ntt_fwd_kernel(Op op, int s0) {
+// The radix-8 shared-memory passes from local stage S on, unrolled at compile time so
+// every index offset is a constant.
+template <int S, int LOGB, int T, bool SIDE, class Op, class Ctx>
+__device__ __forceinline__ void fwd_passes(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
+    if constexpr (S < LOGB) {
+        fwd_pass<3, false, LOGB, T, S, SIDE>(op, c, sm, rbase);
+        fwd_passes<S + 3, LOGB, T, SIDE>(op, c, sm, rbase);
+    }
+}
+
+template <int LOGB, int V, class Op>
+__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op, int s0) {
     extern __shared__ uint64_t sm[];
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB>::THREADS;
-    constexpr int REM = NttCfg<LOGB>::REM;
+    constexpr int T = NttCfg<LOGB, V>::THREADS;
+    constexpr int REM = NttCfg<LOGB, V>::REM;
     const auto c = op.ctx(blockIdx.x);
     const uint32_t rbase = (1u << s0) + c.lm.sb;
-    int s;
-    if constexpr (REM != 0) {
-        fwd_pass<REM, true, LOGB>(op, c, sm, 0, rbase);
-        s = REM;
-    } else {
-        fwd_pass<3, true, LOGB>(op, c, sm, 0, rbase);
-        s = 3;
-    }
-    for (; s < LOGB; s += 3) fwd_pass<3, false, LOGB>(op, c, sm, s, rbase);
+    constexpr int FIRST = REM != 0 ? REM : 3;
+    fwd_pass<FIRST, true, LOGB, T, 0, (V > 0)>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, (V > 0)>(op, c, sm, rbase);
     // coalesced copy-out, two coefficients per thread
     for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
         const int p = swz(e);
@@ -123,59 +152,87 @@ __global__ void __launch_bounds__(NttCfg<LOGB>::THREADS) ntt_fwd_kernel(Op op, i
 // Pass of R_LOG Gentleman-Sande stages starting at local stage s; global stage =
 // local stage (an inverse CTA always owns the low stages). logn is log2 of the full
 // limb length; SCALE folds N^-1 into the pass's last stage.
-template <int R_LOG, bool TO_GLOBAL, bool SCALE, int LOGB, class Op, class Ctx>
-__device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *sm, int s, int logn) {
+template <int R_LOG, bool TO_GLOBAL, bool SCALE, int LOGB, int T, int s, bool SIDE, class Op, class Ctx>
+__device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *sm, int logn) {
     constexpr int R = 1 << R_LOG;
     constexpr int NB = 1 << LOGB;
     constexpr int G = NB >> R_LOG;
-    constexpr int T = NttCfg<LOGB>::THREADS;
+    constexpr int IT = G > 0 ? (G + T - 1) / T : 1;  // groups per thread
+    constexpr int GR = SIDE ? IT : 1;                // groups in flight at once
+    constexpr bool FULL = G > 0 && G % T == 0;
     const uint64_t q = c.lm.q, q2 = q << 1;
     const uint32_t n = 1u << logn;
-    for (int g = threadIdx.x; g < G; g += T) {
-        const int j = g & ((1 << s) - 1);
-        const int blk = g >> s;
-        const int base = (blk << (s + R_LOG)) + j;
-        uint64_t v[R];
 #pragma unroll
-        for (int k = 0; k < R; k++) v[k] = sm[swz(base + (k << s))];
+    for (int i0 = 0; i0 < IT; i0 += GR) {
+        uint64_t v[GR][R];
 #pragma unroll
-        for (int t = 0; t < R_LOG; t++) {
-            const int h = 1 << t;
-            const int sg = s + t;
-            const uint32_t rb = n + 1 - (n >> sg) + (c.lm.sb << (LOGB - sg - 1)) + ((uint32_t)blk << (R_LOG - t - 1));
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const int base = ((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1));
 #pragma unroll
-            for (int k = 0; k < R; k++) {
-                if (k & h) continue;
-                if (SCALE && t == R_LOG - 1) {
-                    uint64_t u = v[k] >= q2 ? v[k] - q2 : v[k];
-                    uint64_t y = v[k + h];
-                    uint64_t sum = u + y;
-                    sum = sum >= q2 ? sum - q2 : sum;
-                    v[k] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
-                    v[k + h] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
-                } else {
-                    const uint32_t ri = rb + (uint32_t)(k >> (t + 1));
-                    gs_butterfly(v[k], v[k + h], __ldg(&c.lm.iroots[ri]), q, q2);
+            for (int k = 0; k < R; k++) v[it][k] = sm[swz(base + (k << s))];
+        }
+#pragma unroll
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const int blk = g >> s;
+#pragma unroll
+            for (int t = 0; t < R_LOG; t++) {
+                const int h = 1 << t;
+                const int sg = s + t;
+                const uint32_t rb =
+                    n + 1 - (n >> sg) + (c.lm.sb << (LOGB - sg - 1)) + ((uint32_t)blk << (R_LOG - t - 1));
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    if (k & h) continue;
+                    if (SCALE && t == R_LOG - 1) {
+                        uint64_t u = v[it][k] >= q2 ? v[it][k] - q2 : v[it][k];
+                        uint64_t y = v[it][k + h];
+                        uint64_t sum = u + y;
+                        sum = sum >= q2 ? sum - q2 : sum;
+                        v[it][k] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
+                        v[it][k + h] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
+                    } else {
+                        const uint32_t ri = rb + (uint32_t)(k >> (t + 1));
+                        gs_butterfly(v[it][k], v[it][k + h], __ldg(&c.lm.iroots[ri]), q, q2);
+                    }
                 }
             }
         }
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-            const int e = base + (k << s);
-            if constexpr (TO_GLOBAL) op.store(c, e, v[k]);
-            else sm[swz(e)] = v[k];
+        for (int it = 0; it < GR; it++) {
+            const int g = threadIdx.x + (i0 + it) * T;
+            if (!FULL && g >= G) continue;
+            const int base = ((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1));
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                const int e = base + (k << s);
+                if constexpr (TO_GLOBAL) op.store(c, e, v[it][k]);
+                else sm[swz(e)] = v[it][k];
+            }
         }
     }
     if constexpr (!TO_GLOBAL) __syncthreads();
 }
 
+// Radix-8 passes P .. PASSES-1 (local stages 3P ..), unrolled at compile time.
+template <int P, int PASSES, int LOGB, int T, bool SIDE, class Op, class Ctx>
+__device__ __forceinline__ void inv_passes(const Op &op, const Ctx &c, uint64_t *sm, int logn) {
+    if constexpr (P < PASSES) {
+        inv_pass<3, false, false, LOGB, T, 3 * P, SIDE>(op, c, sm, logn);
+        inv_passes<P + 1, PASSES, LOGB, T, SIDE>(op, c, sm, logn);
+    }
+}
+
 // scale_last: this CTA's last stage is the transform's last stage (whole limb).
-template <int LOGB, class Op>
-__global__ void __launch_bounds__(NttCfg<LOGB>::THREADS) ntt_inv_kernel(Op op, int logn, int scale_last) {
+template <int LOGB, int V, class Op>
+__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op, int logn, int scale_last) {
     extern __shared__ uint64_t sm[];
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB>::THREADS;
-    constexpr int REM = NttCfg<LOGB>::REM;
+    constexpr int T = NttCfg<LOGB, V>::THREADS;
+    constexpr int REM = NttCfg<LOGB, V>::REM;
     const auto c = op.ctx(blockIdx.x);
     for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
         uint64_t a, b;
@@ -188,11 +245,10 @@ __global__ void __launch_bounds__(NttCfg<LOGB>::THREADS) ntt_inv_kernel(Op op, i
     }
     __syncthreads();
     constexpr int LAST = REM ? REM : 3;
-    constexpr int FULL = REM ? LOGB / 3 : LOGB / 3 - 1;  // radix-8 passes before the last one
-    int s = 0;
-    for (int p = 0; p < FULL; p++, s += 3) inv_pass<3, false, false, LOGB>(op, c, sm, s, logn);
-    if (scale_last) inv_pass<LAST, true, true, LOGB>(op, c, sm, s, logn);
-    else inv_pass<LAST, true, false, LOGB>(op, c, sm, s, logn);
+    constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;  // radix-8 passes before the last one
+    inv_passes<0, PASSES, LOGB, T, (V > 0)>(op, c, sm, logn);
+    if (scale_last) inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, (V > 0)>(op, c, sm, logn);
+    else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, (V > 0)>(op, c, sm, logn);
 }
 
 template <int LOGB>
@@ -215,45 +271,59 @@ __device__ __forceinline__ NttLimb make_limb(const Mod &m, uint32_t sb) {
 
 constexpr int MAX_LOGB = 14;  // 16384 coefficients = 128 KB of shared memory per CTA
 
-template <int LOGB, class Op>
+template <int LOGB, int V, class Op>
 inline cudaError_t launch_fwd(const Op &op, unsigned blocks, int s0, cudaStream_t s) {
     const size_t smem = ntt_smem_bytes<LOGB>();
-    auto k = ntt_fwd_kernel<LOGB, Op>;
+    auto k = ntt_fwd_kernel<LOGB, V, Op>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    k<<<blocks, NttCfg<LOGB>::THREADS, smem, s>>>(op, s0);
+    k<<<blocks, NttCfg<LOGB, V>::THREADS, smem, s>>>(op, s0);
     return cudaGetLastError();
 }
 
-template <int LOGB, class Op>
+template <int LOGB, int V, class Op>
 inline cudaError_t launch_inv(const Op &op, unsigned blocks, int logn, int scale_last, cudaStream_t s) {
     const size_t smem = ntt_smem_bytes<LOGB>();
-    auto k = ntt_inv_kernel<LOGB, Op>;
+    auto k = ntt_inv_kernel<LOGB, V, Op>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    k<<<blocks, NttCfg<LOGB>::THREADS, smem, s>>>(op, logn, scale_last);
+    k<<<blocks, NttCfg<LOGB, V>::THREADS, smem, s>>>(op, logn, scale_last);
     return cudaGetLastError();
 }
 
-// Dispatch on log2 of the CTA block (1 .. 14).
+// Tuned thread-count variant per (direction, log2 block size); 0 = default. Written by
+// the tuner (tune.cu), read at every launch.
+int ntt_variant(bool fwd, int logb);
+
+template <bool FWD, int LOGB, int V, class Op>
+inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
+    if constexpr (FWD) return launch_fwd<LOGB, V>(op, blocks, s0_or_logn, s);
+    else return launch_inv<LOGB, V>(op, blocks, s0_or_logn, scale_last, s);
+}
+
+// Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry a second
+// variant with half the threads.
 template <bool FWD, class Op>
 cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
-#define TB_CASE(B)                                                          \
-    case B:                                                                 \
-        if constexpr (FWD) return launch_fwd<B>(op, blocks, s0_or_logn, s); \
-        else return launch_inv<B>(op, blocks, s0_or_logn, scale_last, s);
+#define TB_CASE(B) \
+    case B:        \
+        return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);
+#define TB_CASE2(B)                                                                                  \
+    case B:                                                                                          \
+        if (ntt_variant(FWD, B) == 1) return launch_ntt<FWD, B, 1>(op, blocks, s0_or_logn, scale_last, s); \
+        return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);
     switch (logb) {
         TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
-        TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE(12) TB_CASE(13) TB_CASE(14)
+        TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE2(12) TB_CASE2(13) TB_CASE2(14)
     default:
         return cudaErrorInvalidValue;
     }
 #undef TB_CASE
+#undef TB_CASE2
 }
-
 
 }  // namespace tb

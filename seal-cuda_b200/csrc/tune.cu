@@ -1,0 +1,130 @@
+// Tuning knobs and the autotuner.
+//
+// Knobs: the NTT thread-count variant per (direction, log2 block size) and the key-
+// switch scratch budget (how many ciphertexts one key-switch launch sequence takes).
+// The autotuner times the candidates of a knob on the caller's device with CUDA
+// events on scratch data and keeps the fastest; results are process-wide. All
+// variants compute identical words, so tuning changes speed only.
+#include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <vector>
+
+#include "../../include/troy_b200.h"
+#include "context.hpp"
+#include "ntt.cuh"
+
+namespace tb {
+
+namespace {
+std::atomic<int> g_variant[2][MAX_LOGB + 1];
+std::atomic<unsigned long long> g_ks_budget{0};
+}  // namespace
+
+int ntt_variant(bool fwd, int logb) {
+    if (logb < 0 || logb > MAX_LOGB) return 0;
+    return g_variant[fwd ? 1 : 0][logb].load(std::memory_order_relaxed);
+}
+
+size_t ks_scratch_budget() {
+    unsigned long long v = g_ks_budget.load(std::memory_order_relaxed);
+    if (v) return (size_t)v;
+    const char *e = getenv("TB_KS_SCRATCH_BYTES");
+    return e ? (size_t)strtoull(e, nullptr, 10) : (size_t)(2ull << 30);
+}
+
+int ntt_forward(const Context &c, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, bool lazy,
+                cudaStream_t s);
+int ntt_inverse(const Context &c, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, bool lazy,
+                cudaStream_t s);
+
+// Median device time of `reps` calls of f after one warm-up call.
+template <class F>
+static float time_call(F &&f, cudaStream_t s, int reps, int &status) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    std::vector<float> ms;
+    status = f();
+    for (int r = 0; r < reps && status == TB_OK; r++) {
+        cudaEventRecord(a, s);
+        status = f();
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float t = 0;
+        cudaEventElapsedTime(&t, a, b);
+        ms.push_back(t);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms.empty()) return 0;
+    std::sort(ms.begin(), ms.end());
+    return ms[ms.size() / 2];
+}
+
+// Times both variants of the forward and inverse transform of the context's degree
+// on `polys` limbs of scratch and keeps the faster of each.
+int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, int *chosen_inv) {
+    const int logb = c.logn;
+    if (logb < 12 || logb > MAX_LOGB) {
+        if (chosen_fwd) *chosen_fwd = 0;
+        if (chosen_inv) *chosen_inv = 0;
+        return TB_OK;  // one variant only
+    }
+    if (!polys) polys = 256;
+    const int limbs = (int)std::min<size_t>(c.chain.size(), polys);
+    const uint64_t P = (polys + limbs - 1) / limbs;
+    uint64_t *buf = nullptr;
+    cudaError_t e = cudaMallocAsync(&buf, 8ull * P * limbs * c.n, s);
+    if (e != cudaSuccess) return status_from(e);
+    e = cudaMemsetAsync(buf, 0, 8ull * P * limbs * c.n, s);
+    int st = e == cudaSuccess ? TB_OK : status_from(e);
+    for (int dir = 1; dir >= 0 && st == TB_OK; dir--) {
+        float best = 0;
+        int best_v = 0;
+        for (int v = 0; v <= 1 && st == TB_OK; v++) {
+            g_variant[dir][logb].store(v);
+            const float t = time_call(
+                [&] {
+                    return dir ? ntt_forward(c, buf, buf, P, 0, limbs, false, s)
+                               : ntt_inverse(c, buf, buf, P, 0, limbs, false, s);
+                },
+                s, 5, st);
+            if (st == TB_OK && (v == 0 || t < best)) {
+                best = t;
+                best_v = v;
+            }
+        }
+        g_variant[dir][logb].store(best_v);
+        if (dir && chosen_fwd) *chosen_fwd = best_v;
+        if (!dir && chosen_inv) *chosen_inv = best_v;
+    }
+    cudaFreeAsync(buf, s);
+    return st;
+}
+
+}  // namespace tb
+
+extern "C" {
+
+int tb_ntt_set_variant(int forward, int log_block, int variant) {
+    if (log_block < 1 || log_block > tb::MAX_LOGB || variant < 0 || variant > 1 || (variant && log_block < 12))
+        return tb::set_error(TB_ERR_INVALID_ARGUMENT, "no such NTT variant");
+    tb::g_variant[forward ? 1 : 0][log_block].store(variant);
+    return TB_OK;
+}
+
+int tb_ntt_get_variant(int forward, int log_block, int *variant) {
+    if (!variant || log_block < 1 || log_block > tb::MAX_LOGB) return tb::set_error(TB_ERR_INVALID_ARGUMENT, "bad block");
+    *variant = tb::ntt_variant(forward != 0, log_block);
+    return TB_OK;
+}
+
+int tb_keyswitch_set_budget(uint64_t bytes) {
+    tb::g_ks_budget.store(bytes);
+    return TB_OK;
+}
+
+uint64_t tb_keyswitch_get_budget(void) { return tb::ks_scratch_budget(); }
+
+}  // extern "C"

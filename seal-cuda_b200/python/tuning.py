@@ -1,0 +1,51 @@
+"""Workload-level autotuner over the library's speed knobs.
+
+The library's knobs (include/troy_b200.h, "tuning"): the NTT launch variant per
+direction for 2^12..2^14 blocks and the key-switch scratch budget (how many
+ciphertexts one key-switch launch sequence takes). Every setting computes the same
+words, so the tuner may pick any of them: it times the caller's own step function
+with CUDA events under each candidate setting and keeps the fastest. Results are
+process-wide settings of the library.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+
+import tb_capi
+
+
+def _set(logn, fwd, inv, budget):
+    lib = tb_capi.lib()
+    if 12 <= logn <= 14:
+        tb_capi.check(lib.tb_ntt_set_variant(1, logn, fwd))
+        tb_capi.check(lib.tb_ntt_set_variant(0, logn, inv))
+    lib.tb_keyswitch_set_budget.argtypes = [ctypes.c_uint64]
+    tb_capi.check(lib.tb_keyswitch_set_budget(budget))
+
+
+def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
+    """Times `step()` (which launches one workload step on `stream`, a torch stream)
+    under each combination of NTT variants and key-switch budget (0 = the default),
+    keeps the fastest setting and returns {"forward", "inverse", "ks_budget", "ms",
+    "default_ms"}."""
+    import torch
+
+    variants = (0, 1) if 12 <= logn <= 14 else (0,)
+    results = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for fwd, inv, budget in itertools.product(variants, variants, budgets):
+        _set(logn, fwd, inv, budget)
+        step()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        results.append((e0.elapsed_time(e1) / reps, fwd, inv, budget))
+    default_ms = next(r[0] for r in results if r[1:] == (0, 0, 0))
+    ms, fwd, inv, budget = min(results)
+    _set(logn, fwd, inv, budget)
+    return {"forward": fwd, "inverse": inv, "ks_budget": budget or "default", "ms": round(ms, 4),
+            "default_ms": round(default_ms, 4)}

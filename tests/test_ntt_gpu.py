@@ -94,3 +94,39 @@ def test_batched_ntt_sweep_shapes(orc):
         ey = orc.ntt_forward_rns(logn, moduli, y)
         ez = orc.ntt_inverse_rns(logn, moduli, orc.dyadic_rns(moduli, ex, ey))
         assert np.array_equal(_host(dz), ez), n
+
+
+@pytest.mark.parametrize("logn", [12, 13, 14, 15, 16])
+def test_ntt_launch_variants_are_identical(orc, logn):
+    """Both thread-count variants of the 2^12..2^14 block kernels (also used inside the
+    split transform of longer limbs) give the oracle's words, and the autotuner keeps a
+    valid choice."""
+    lib = tb_capi.lib()
+    n = 1 << logn
+    moduli = orc.coeff_modulus_create(n, [50, 50, 40])
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(100 + logn)
+    x = np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli])[None]
+    d = _dev(x)
+    out = torch.empty_like(d)
+    exp_f = orc.ntt_forward_rns(logn, moduli, x, lazy=False)
+    exp_i = orc.ntt_inverse_rns(logn, moduli, x, lazy=False)
+    try:
+        for v in (0, 1):
+            for b in (12, 13, 14):
+                tb_capi.check(lib.tb_ntt_set_variant(1, b, v))
+                tb_capi.check(lib.tb_ntt_set_variant(0, b, v))
+            ctx("ntt_forward", d, out, 1, 0, len(moduli), 0, None)
+            assert np.array_equal(_host(out), exp_f), v
+            ctx("ntt_inverse", d, out, 1, 0, len(moduli), 0, None)
+            assert np.array_equal(_host(out), exp_i), v
+        import ctypes
+        f, i = ctypes.c_int(-1), ctypes.c_int(-1)
+        ctx("autotune_ntt", 64, None, ctypes.byref(f), ctypes.byref(i))
+        assert f.value in (0, 1) and i.value in (0, 1)
+        ctx("ntt_forward", d, out, 1, 0, len(moduli), 0, None)
+        assert np.array_equal(_host(out), exp_f)
+    finally:
+        for b in (12, 13, 14):
+            lib.tb_ntt_set_variant(1, b, 0)
+            lib.tb_ntt_set_variant(0, b, 0)

@@ -259,7 +259,10 @@ def test_ckks_encoder_and_evaluator_surface():
     w = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
     cv, cw = encryptor.encrypt(enc.encode(v, scale)), encryptor.encrypt(enc.encode(w, scale))
     d = lambda c: enc.decode(dec.decrypt(c))
-    tol = 2.0 ** -20
+    # against the FP64 plaintext result the encryption noise counts too (about 2^-20
+    # at scale 2^40 after a key switch); the 2^-20 bound vs the reference's decode of
+    # the same ciphertext is checked in test_ckks_seeded_chain_matches_reference
+    tol = 2.0 ** -17
     assert np.abs(d(ev.add(cv, cw)) - (v + w)).max() < tol
     assert np.abs(d(ev.sub(cv, cw)) - (v - w)).max() < tol
     assert np.abs(d(ev.negate(cv)) + v).max() < tol
