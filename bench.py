@@ -19,6 +19,9 @@ prime (the arithmetic performed is the same as on encrypted data).
   oracle/_ref) on a bounded sample of the same workload, one process per core.
 * ``plain_per_op``: the same chain driven one pair per call (batch 1), as the
   reference's evaluator is used; ``batched_over_per_op`` is the batching gain.
+* ``uneven_batch``: 512 BFV/BGV ciphertexts of degrees 4096 / 8192 / 16384 through
+  multiply, relinearize and rotate_rows as one captured CUDA graph, beside the
+  one-ciphertext-per-call path.
 * ``serving``: the serving loop (MatmulServer, BFV N = 8192, 5 primes): Poisson
   arrivals of encrypted vector x matrix requests at several rates plus a burst,
   p50/p99 latency and throughput per rate.
@@ -273,6 +276,67 @@ def run_b200(args, rank, world):
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
 
 
+UNEVEN_SHAPES = [(1, 4096, [36, 36, 37]), (3, 8192, [43, 43, 44, 44, 44]), (1, 16384, [48] * 9)]
+
+
+def run_uneven(total=512, reps=5):
+    """The uneven-batch workload: `total` ciphertext pairs whose ring degree is drawn from
+    {4096, 8192, 16384} (3 / 5 / 9 primes; BFV, BGV, BFV), multiply -> relinearize ->
+    rotate_rows(1), seeded uniform residues as ciphertexts and keys. Reports ops/s of
+    the captured CUDA graph (one launch per batch), of the stream-overlapped calls and
+    of the one-ciphertext-per-call path."""
+    import numpy as np
+    import torch
+    import tb_capi
+    from uneven import ShapeGroup, UnevenBatch
+
+    rng = np.random.default_rng(4096)
+    draws = rng.integers(0, len(UNEVEN_SHAPES), total)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(99)
+    lib = tb_capi.lib()
+    groups = []
+    for gi, (scheme, n, bits) in enumerate(UNEVEN_SHAPES):
+        arr = (ctypes.c_int * len(bits))(*bits)
+        mods = (ctypes.c_uint64 * len(bits))()
+        tb_capi.check(lib.tb_coeff_modulus_create(ctypes.c_uint64(n), arr, len(bits), mods))
+        moduli = [int(m) for m in mods]
+        tmod = ctypes.c_uint64()
+        tb_capi.check(lib.tb_plain_modulus_batching(ctypes.c_uint64(16384), 20, ctypes.byref(tmod)))
+        ctx = tb_capi.Context(scheme, n, moduli, tmod.value)
+        K, L, cnt = len(moduli), len(moduli) - 1, int((draws == gi).sum())
+        e = ctypes.c_uint32()
+        ctx("galois_elt_from_step", 1, ctypes.byref(e))
+        groups.append(ShapeGroup(ctx, L, _rand_residues(torch, (cnt, 2, L, n), moduli[:L], gen),
+                                 _rand_residues(torch, (cnt, 2, L, n), moduli[:L], gen),
+                                 _rand_residues(torch, (K - 1, 2, K, n), moduli, gen),
+                                 _rand_residues(torch, (K - 1, 2, K, n), moduli, gen), e.value))
+    batch = UnevenBatch(groups)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    ms_streams = timed(batch.run, reps)
+    ms_per_op = timed(batch.run_per_op, 1)
+    batch.capture()
+    ms_graph = timed(batch.replay, reps)
+    return {"workload": "uneven_bfv_bgv_n4096_8192_16384_mul_relin_rotate", "ciphertexts": total,
+            "groups": {f"N={g.ctx.n},L={g.L}": g.count for g in groups},
+            "graph_ops_per_s": round(total / (ms_graph * 1e-3), 1),
+            "streams_ops_per_s": round(total / (ms_streams * 1e-3), 1),
+            "per_op_ops_per_s": round(total / (ms_per_op * 1e-3), 1),
+            "graph_over_per_op": round(ms_per_op / ms_graph, 2)}
+
+
 def _pinned(a):
     """A page-locked copy of a uint64 array (what a server's receive buffers would be)."""
     import numpy as np
@@ -490,6 +554,7 @@ def main():
     ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker in the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
                     help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
@@ -541,6 +606,7 @@ def main():
                    "sample": f"{ops} ops ({args.cpu_ops} per process x {workers} processes), {busy:.1f} s"}
         per_op = 1e3 / res["per_op_ms"]
         serving = None if args.no_serving else run_serving()
+        uneven = None if args.no_uneven else run_uneven()
         line = {"metric": METRIC, "value": round(value, 2), "unit": "ops/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(res["ms"], 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact modular)",
@@ -557,6 +623,7 @@ def main():
                                  "form": "one pair per call chain (batch 1), same kernels and keys",
                                  "batched_over_per_op": round(value / (per_op * world), 2)},
                 "serving": serving,
+                "uneven_batch": uneven,
                 "clocks": res["clocks"],
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(res["trace"].items())}}
         print(json.dumps(line))
