@@ -379,11 +379,15 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
         h = pytroy.MatmulHelper(1, inp, out, SERVE_N)
         cts = h.encrypt_inputs(encryptor, enc, x)
         words = np.concatenate([np.asarray(c.data(), np.uint64) for c in cts[0]])
-        pool.append((inp, out, _pinned(words), _pinned(w)))
+        # page-locked request and result buffers, as a server's receive/send buffers;
+        # requests sharing a pool entry overwrite its result buffer (values not read here)
+        blocks = (out + h.output_block - 1) // h.output_block
+        res = _pinned(np.zeros(blocks * 2 * (len(SERVE_BITS) - 1) * SERVE_N, np.uint64))
+        pool.append((inp, out, _pinned(words), _pinned(w), res))
     server = pytroy.MatmulServer(ctx, memory_budget=16 << 30, slots=3)
     now = pytroy.MatmulServer.now
     for r in pool[:8]:  # warm-up
-        server.submit(r[0], r[1], r[2], r[3], now())
+        server.submit(r[0], r[1], r[2], r[3], now(), outputs=r[4])
     server.drain(60.0)
 
     def run(rate):
@@ -392,12 +396,13 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
         start = now()
         due = start + np.cumsum(gaps)
         ids, k = [], 0
-        waves0 = server.stats()["waves"]
+        st0 = server.stats()
+        waves0 = st0["waves"]
         while k < count or not server.idle():
             tnow = now()
             while k < count and due[k] <= tnow:
                 r = pool[k % len(pool)]
-                ids.append(server.submit(r[0], r[1], r[2], r[3], float(due[k])))
+                ids.append(server.submit(r[0], r[1], r[2], r[3], float(due[k]), outputs=r[4]))
                 k += 1
             server.step()
             if tnow - start > 120.0:
@@ -409,10 +414,13 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
             lat.append(1e3 * (done - arrival))
             first = arrival if first is None else min(first, arrival)
             last = done if last is None else max(last, done)
-        waves = server.stats()["waves"] - waves0
+        st = server.stats()
+        waves = st["waves"] - waves0
+        host = {k: round(st[k] - st0[k], 4) for k in ("launch_host_s", "reap_host_s", "device_s")}
         return {"rate_rps": rate if rate is not None else "burst", "requests": count, "ok": ok,
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                "throughput_rps": round(count / (last - first), 1), "mean_wave": round(count / max(1, waves), 2)}
+                "throughput_rps": round(count / (last - first), 1), "mean_wave": round(count / max(1, waves), 2),
+                "server_seconds": host}
 
     runs = [run(r) for r in SERVE_RATES] + [run(None)]
     return {"workload": "bfv_n8192_L4_matmul_poisson", "slots": 3, "memory_budget_gb": 16,

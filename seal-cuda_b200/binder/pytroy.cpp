@@ -542,14 +542,32 @@ PYBIND11_MODULE(pytroy, m) {
              py::arg("max_wave_requests") = 256, py::arg("output_staging") = std::size_t(256) << 20,
              py::keep_alive<1, 2>())
         .def_static("now", &MatmulServer::now)
-        .def("submit",
-             [](MatmulServer &s, std::size_t in, std::size_t out, U64Array inputs, U64Array weights, double arrival) {
-                 if ((std::size_t)weights.size() != in * out) throw std::invalid_argument("Weight size incorrect.");
-                 // the arrays are read at admission; holding them here keeps them alive
-                 // (requests are admitted and released inside step(), with the GIL held)
-                 auto owner = std::make_shared<std::pair<U64Array, U64Array>>(inputs, weights);
-                 return s.submitBorrowed(in, out, inputs.data(), inputs.size(), weights.data(), arrival, owner);
-             })
+        .def(
+            "submit",
+            [](MatmulServer &s, std::size_t in, std::size_t out, U64Array inputs, U64Array weights, double arrival,
+               py::object outputs) {
+                if ((std::size_t)weights.size() != in * out) throw std::invalid_argument("Weight size incorrect.");
+                uint64_t *dst = nullptr;
+                py::array out_arr;
+                if (!outputs.is_none()) {  // written in place: no conversion, no copy
+                    if (!py::isinstance<py::array>(outputs)) throw std::invalid_argument("outputs must be an array");
+                    out_arr = outputs.cast<py::array>();
+                    if (!out_arr.dtype().is(py::dtype::of<uint64_t>()) || !(out_arr.flags() & py::array::c_style) ||
+                        !out_arr.writeable())
+                        throw std::invalid_argument("outputs must be a writable contiguous uint64 array");
+                    const MatmulPlan p = MatmulPlan::make(1, in, out, s.slotDegree());
+                    if ((std::size_t)out_arr.size() != p.outputBlocks() * s.ciphertextWords())
+                        throw std::invalid_argument("outputs size incorrect.");
+                    dst = static_cast<uint64_t *>(out_arr.mutable_data());
+                }
+                // the arrays are read at admission and written at completion; holding them
+                // here keeps them alive (requests are admitted and finished inside step(),
+                // with the GIL held)
+                auto owner = std::make_shared<std::tuple<U64Array, U64Array, py::array>>(inputs, weights, out_arr);
+                return s.submitBorrowed(in, out, inputs.data(), inputs.size(), weights.data(), arrival, owner, dst);
+            },
+            py::arg("in_dims"), py::arg("out_dims"), py::arg("inputs"), py::arg("weights"), py::arg("arrival"),
+            py::arg("outputs") = py::none())
         .def("step", &MatmulServer::step)
         .def("drain", &MatmulServer::drain)
         .def("idle", &MatmulServer::idle)

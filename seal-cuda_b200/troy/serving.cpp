@@ -318,7 +318,8 @@ std::size_t MatmulServer::footprint(const MatmulPlan &p) const {
 }
 
 uint64_t MatmulServer::submitBorrowed(std::size_t in, std::size_t out, const uint64_t *inputs, std::size_t input_words,
-                                      const uint64_t *weights, double arrival, std::shared_ptr<void> owner) {
+                                      const uint64_t *weights, double arrival, std::shared_ptr<void> owner,
+                                      uint64_t *outputs) {
     MatmulPlan p = MatmulPlan::make(1, in, out, n_);
     const std::size_t ctw = 2 * (std::size_t)L_ * n_;
     if (input_words != p.inputBlocks() * ctw) throw std::invalid_argument("input ciphertext words do not match the shape");
@@ -332,6 +333,8 @@ uint64_t MatmulServer::submitBorrowed(std::size_t in, std::size_t out, const uin
     r.w_ptr = weights;
     r.owner = std::move(owner);
     r.pinned = is_pinned(inputs) && is_pinned(weights);
+    r.out_ptr = outputs;
+    r.out_pinned = outputs && is_pinned(outputs);
     r.arrival = arrival;
     r.bytes = footprint(p);
     if (r.bytes > opt_.memory_budget) throw std::invalid_argument("request larger than the memory budget");
@@ -419,7 +422,7 @@ bool MatmulServer::launch(int slot) {
             std::memcpy(h + hs, r.w_ptr, ww * 8);
             src_w.push_back(h + hs);
             hs += ww * 8;
-            r.owner.reset();  // staged; the borrowed memory may go
+            if (!r.out_ptr) r.owner.reset();  // staged; the borrowed memory may go
         }
     }
 
@@ -458,8 +461,14 @@ bool MatmulServer::launch(int slot) {
         st = tb_dyadic_accumulate(hctx, L_, 2, U(o_in), 0, U(o_wn), 0, U(o_out), 0, V(o_off), V(o_ia), V(o_iw),
                                   (uint32_t)no, s);
     if (st == TB_OK) st = tb_ntt_inverse(hctx, U(o_out), U(o_out), 2 * no, 0, L_, 0, s);
-    if (st == TB_OK && cudaMemcpyAsync(pin_out.p, U(o_out), no * ctw * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-        st = TB_ERR_CUDA;
+    // results: straight into page-locked caller buffers, the rest through the staging
+    for (std::size_t k = 0; k < w->reqs.size() && st == TB_OK; k++) {
+        const Request &r = w->reqs[k];
+        const std::size_t words = r.plan.outputBlocks() * ctw;
+        void *dst = r.out_pinned ? (void *)r.out_ptr : (void *)(static_cast<uint64_t *>(pin_out.p) + w->out_base[k] * ctw);
+        if (cudaMemcpyAsync(dst, U(o_out) + w->out_base[k] * ctw, words * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            st = TB_ERR_CUDA;
+    }
     w->failed = st != TB_OK;
     if (w->dev) cudaFreeAsync(w->dev, s);
     cuda_ok(cudaEventRecord(w->done, s), "event record");
@@ -491,7 +500,10 @@ void MatmulServer::reap(std::vector<uint64_t> &finished) {
             d.ok = ok;
             if (ok) {
                 const std::size_t words = r.plan.outputBlocks() * ctw;
-                d.outputs.assign(out + w.out_base[k] * ctw, out + w.out_base[k] * ctw + words);
+                if (!r.out_ptr)
+                    d.outputs.assign(out + w.out_base[k] * ctw, out + w.out_base[k] * ctw + words);
+                else if (!r.out_pinned)
+                    std::memcpy(r.out_ptr, out + w.out_base[k] * ctw, words * 8);
             }
             done_[r.id] = std::move(d);
             finished.push_back(r.id);

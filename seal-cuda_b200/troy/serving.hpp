@@ -92,9 +92,11 @@ public:
     // request is admitted, and `owner` (may be null) is held until they have been read;
     // the caller keeps the memory unchanged meanwhile. Page-locked (pinned) memory is
     // copied to the device directly; other memory goes through the slot's staging.
+    // With `outputs` (plan.outputBlocks() x 2 x L x N words, page-locked for a direct
+    // copy) the results are written there and result()/take() hand back no words.
     std::uint64_t submitBorrowed(std::size_t in, std::size_t out, const std::uint64_t *inputs,
                                  std::size_t input_words, const std::uint64_t *weights, double arrival,
-                                 std::shared_ptr<void> owner);
+                                 std::shared_ptr<void> owner, std::uint64_t *outputs = nullptr);
     // Non-blocking: collects finished waves, then launches new waves on free slots.
     // Returns the ids that finished during this call.
     std::vector<std::uint64_t> step();
@@ -102,6 +104,8 @@ public:
     // passed; returns false on timeout.
     bool drain(double timeout);
     bool idle() const { return queue_.empty() && running_.empty(); }
+    std::size_t slotDegree() const { return n_; }
+    std::size_t ciphertextWords() const { return 2 * (std::size_t)L_ * n_; }
     std::size_t queued() const { return queue_.size(); }
     // Output ciphertexts (plan.outputBlocks() x 2 x L x N words) of a finished request,
     // with its arrival and completion stamps; false if unknown or not finished.
@@ -123,6 +127,8 @@ private:
         const std::uint64_t *in_ptr = nullptr, *w_ptr = nullptr;
         std::shared_ptr<void> owner;                  // keeps borrowed memory alive
         bool pinned = false;                          // both arrays page-locked: direct copies
+        std::uint64_t *out_ptr = nullptr;             // caller's result buffer, if any
+        bool out_pinned = false;
         double arrival;
         std::size_t bytes;
     };

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
 pytroy = pytest.importorskip("pytroy")
 from oracle import RefSession, available  # noqa: E402
 
@@ -119,7 +120,14 @@ def _run_alone(ns, server):
     return outs
 
 
-def _run_poisson(ns, server, rate, seed):
+def _out_buffer(k, size):
+    """Result buffers given to the server: plain memory for even k, page-locked for odd."""
+    if k % 2 == 0:
+        return np.zeros(size, np.uint64)
+    return torch.zeros(size, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+
+
+def _run_poisson(ns, server, rate, seed, outs=None):
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, len(ns.reqs))
     start = pytroy.MatmulServer.now()
@@ -130,7 +138,8 @@ def _run_poisson(ns, server, rate, seed):
         now = pytroy.MatmulServer.now()
         while k < len(ns.reqs) and due[k] <= now:
             inp, out, x, w, h, cts, words = ns.reqs[k]
-            ids.append(server.submit(inp, out, words, w, float(due[k])))
+            dst = None if outs is None else outs[k]
+            ids.append(server.submit(inp, out, words, w, float(due[k]), outputs=dst))
             k += 1
         server.step()
         assert now < deadline
@@ -146,6 +155,14 @@ def test_server_results_identical_alone_and_in_the_mix(serving):
     assert st["completed"] == len(ns.reqs) and st["failed"] == 0
     assert st["max_wave"] > 1  # requests really were batched together
     L = len(BITS) - 1
+    # the same stream with caller-owned result buffers (plain and page-locked memory)
+    outs = [_out_buffer(k, a.size) for k, a in enumerate(alone)]
+    server2 = pytroy.MatmulServer(ns.ctx, slots=3)
+    ids2 = _run_poisson(ns, server2, rate=5000.0, seed=4, outs=outs)
+    for k, rid in enumerate(ids2):
+        o, _, _, ok = server2.take(rid)
+        assert ok and np.asarray(o).size == 0
+        assert np.array_equal(outs[k], alone[k]), k
     for k, rid in enumerate(ids):
         o, arrival, done, ok = server.result(rid)
         assert ok and done >= arrival
