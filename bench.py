@@ -19,6 +19,8 @@ prime (the arithmetic performed is the same as on encrypted data).
   oracle/_ref) on a bounded sample of the same workload, one process per core.
 * ``plain_per_op``: the same chain driven one pair per call (batch 1), as the
   reference's evaluator is used; ``batched_over_per_op`` is the batching gain.
+* ``ntt_sweep``: the raw NTT / dyadic / inverse NTT workload (256 x 8 limbs, N =
+  4096 .. 32768) with GB/s and fraction of the measured copy peak per kernel.
 * ``uneven_batch``: 512 BFV/BGV ciphertexts of degrees 4096 / 8192 / 16384 through
   multiply, relinearize and rotate_rows as one captured CUDA graph, beside the
   one-ciphertext-per-call path.
@@ -274,6 +276,57 @@ def run_b200(args, rank, world):
     return {"tuned": tuned,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
+
+
+def run_ntt_sweep(batch=256, reps=10):
+    """The raw transform workload: `batch` polynomials x 8 limbs of 50-bit primes,
+    N in {4096, ..., 32768}: forward NTT, dyadic product of pairs, inverse NTT.
+    Algorithmic bytes: 16 N B L per transform (read + write), 24 N B L per dyadic
+    product; GB/s and the fraction of the measured copy peak per kernel."""
+    import torch
+    import tb_capi
+
+    lib = tb_capi.lib()
+    peak, _ = _peak_hbm()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(8)
+    out = {}
+    for logn in (12, 13, 14, 15):
+        n = 1 << logn
+        arr = (ctypes.c_int * 8)(*([50] * 8))
+        mods = (ctypes.c_uint64 * 8)()
+        tb_capi.check(lib.tb_coeff_modulus_create(ctypes.c_uint64(n), arr, 8, mods))
+        moduli = [int(m) for m in mods]
+        ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+        x = _rand_residues(torch, (batch, 8, n), moduli, gen)
+        y = _rand_residues(torch, (batch, 8, n), moduli, gen)
+        z = torch.empty_like(x)
+
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        words = batch * 8 * n
+        ms_f = timed(lambda: ctx("ntt_forward", x, x, batch, 0, 8, 0, stream))
+        ms_d = timed(lambda: ctx("dyadic_product", x, y, z, batch, 0, 8, stream))
+        ms_i = timed(lambda: ctx("ntt_inverse", z, z, batch, 0, 8, 0, stream))
+        row = {}
+        for name, ms, bytes_ in (("ntt_forward", ms_f, 16 * words), ("dyadic", ms_d, 24 * words),
+                                 ("ntt_inverse", ms_i, 16 * words)):
+            gbs = bytes_ / (ms * 1e-3) / 1e9
+            row[name] = {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4)}
+        out[f"N={n}"] = row
+        del x, y, z
+        ctx.close()
+    return {"workload": f"{batch} polynomials x 8 limbs (50-bit primes)", "results": out}
 
 
 UNEVEN_SHAPES = [(1, 4096, [36, 36, 37]), (3, 8192, [43, 43, 44, 44, 44]), (1, 16384, [48] * 9)]
@@ -563,6 +616,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
+    ap.add_argument("--no-ntt-sweep", action="store_true", help="skip the raw transform sweep")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
                     help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
@@ -615,6 +669,7 @@ def main():
         per_op = 1e3 / res["per_op_ms"]
         serving = None if args.no_serving else run_serving()
         uneven = None if args.no_uneven else run_uneven()
+        sweep = None if args.no_ntt_sweep else run_ntt_sweep()
         line = {"metric": METRIC, "value": round(value, 2), "unit": "ops/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(res["ms"], 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact modular)",
@@ -632,6 +687,7 @@ def main():
                                  "batched_over_per_op": round(value / (per_op * world), 2)},
                 "serving": serving,
                 "uneven_batch": uneven,
+                "ntt_sweep": sweep,
                 "clocks": res["clocks"],
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(res["trace"].items())}}
         print(json.dumps(line))

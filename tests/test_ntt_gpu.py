@@ -130,3 +130,49 @@ def test_ntt_launch_variants_are_identical(orc, logn):
         for b in (12, 13, 14):
             lib.tb_ntt_set_variant(1, b, 0)
             lib.tb_ntt_set_variant(0, b, 0)
+
+
+@pytest.mark.parametrize("logn", [12, 13, 14, 15])
+def test_raw_ntt_dyadic_sweep_configuration(orc, logn):
+    """The raw NTT / dyadic / inverse NTT workload: L = 8 distinct 50-bit primes
+    = 1 mod 2N, batches of 1 and 16 polynomials checked word for word against the
+    oracle (forward, dyadic product of pairs, inverse); a batch of 256 checked by
+    size-independent properties (round trip, linearity of the transform) and spot
+    polynomials against the oracle."""
+    n = 1 << logn
+    moduli = orc.coeff_modulus_create(n, [50] * 8)
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(7000 + logn)
+
+    def rand(b):
+        return np.stack([np.stack([rng.integers(0, q, n, dtype=np.uint64) for q in moduli]) for _ in range(b)])
+
+    for B in (1, 16):
+        x, y = rand(B), rand(B)
+        dx, dy = _dev(x), _dev(y)
+        ctx("ntt_forward", dx, dx, B, 0, 8, 0, None)
+        ctx("ntt_forward", dy, dy, B, 0, 8, 0, None)
+        fx = orc.ntt_forward_rns(logn, moduli, x)
+        assert np.array_equal(_host(dx), fx)
+        z = torch.empty_like(dx)
+        ctx("dyadic_product", dx, dy, z, B, 0, 8, None)
+        fz = np.stack([orc.dyadic_rns(moduli, fx[b], orc.ntt_forward_rns(logn, moduli, y[b:b + 1])[0])
+                       for b in range(B)])
+        assert np.array_equal(_host(z), fz)
+        ctx("ntt_inverse", z, z, B, 0, 8, 0, None)
+        assert np.array_equal(_host(z), orc.ntt_inverse_rns(logn, moduli, fz))
+    B = 256 if logn <= 14 else 64
+    x = torch.remainder(torch.randint(0, 2 ** 62, (B, 8, n), dtype=torch.int64, device="cuda"),
+                        torch.tensor(moduli, dtype=torch.int64, device="cuda").view(8, 1))
+    y = x.clone()
+    ctx("ntt_forward", y, y, B, 0, 8, 0, None)
+    for b in (0, B // 2, B - 1):
+        assert np.array_equal(_host(y[b]), orc.ntt_forward_rns(logn, moduli, _host(x[b])[None])[0])
+    # linearity: NTT(x + x') = NTT(x) + NTT(x') limb-wise mod q
+    x2 = torch.roll(x, 1, 0)
+    s = torch.remainder(x + x2, torch.tensor(moduli, dtype=torch.int64, device="cuda").view(8, 1))
+    ctx("ntt_forward", s, s, B, 0, 8, 0, None)
+    y2 = torch.roll(y, 1, 0)
+    assert torch.equal(s, torch.remainder(y + y2, torch.tensor(moduli, dtype=torch.int64, device="cuda").view(8, 1)))
+    ctx("ntt_inverse", y, y, B, 0, 8, 0, None)
+    assert torch.equal(y, x)
