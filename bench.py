@@ -19,6 +19,9 @@ prime (the arithmetic performed is the same as on encrypted data).
   oracle/_ref) on a bounded sample of the same workload, one process per core.
 * ``plain_per_op``: the same chain driven one pair per call (batch 1), as the
   reference's evaluator is used; ``batched_over_per_op`` is the batching gain.
+* ``reference_gpu_per_op``: the reference's own CUDA evaluator (its sources compiled
+  for sm_100a under oracle/_ref by oracle/Makefile) on the same workload, one pair
+  per call, in a child process; ``batched_over_reference_gpu_per_op`` compares.
 * ``ntt_sweep``: the raw NTT / dyadic / inverse NTT workload (256 x 8 limbs, N =
   4096 .. 32768) with GB/s and fraction of the measured copy peak per kernel.
 * ``uneven_batch``: 512 BFV/BGV ciphertexts of degrees 4096 / 8192 / 16384 through
@@ -597,6 +600,41 @@ def cpu_reference(ops_per_worker, workers):
     return ops / busy, ops, busy, wall
 
 
+def _ref_gpu_worker(args):
+    """Child process: the reference's own CUDA evaluator (oracle/_ref/libtroyref_gpu.so)
+    one pair per call; its stdout prints are discarded."""
+    ops, = args
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libtroyref_gpu.so"))
+    lib.ref_gpu_ckks_chain.argtypes = [ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    moduli = _ref_moduli()
+    arr = (ctypes.c_uint64 * len(moduli))(*moduli)
+    st = (ctypes.c_int * len(STEPS_K))(*STEPS_K)
+    ms, err = ctypes.c_double(), ctypes.c_double()
+    rc = lib.ref_gpu_ckks_chain(N, arr, len(moduli), SCALE_BITS, ops, st, len(STEPS_K), ctypes.byref(ms),
+                                ctypes.byref(err))
+    return rc, ms.value, err.value
+
+
+def reference_gpu_per_op(ops=16):
+    """ops/s of the reference's CUDA path (compiled for sm_100a from its sources by
+    oracle/Makefile) on this workload, one pair per call chain, as the reference is
+    used; None when that library is not built."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libtroyref_gpu.so")):
+        return None
+    with mp.get_context("spawn").Pool(1) as pool:
+        rc, ms, err = pool.apply(_ref_gpu_worker, ((ops,),))
+    if rc == 1 or ms <= 0:
+        return {"unavailable": "reference CUDA path raised an exception"}
+    return {"value": round(1e3 / ms, 2), "unit": "ops/s", "ms_per_op": round(ms, 3), "ops": ops,
+            "max_abs_error_vs_fp64": err,
+            "note": "reference EvaluatorCuda compiled for sm_100a; pending CUDA error after the run" if rc == 2
+            else "reference EvaluatorCuda compiled for sm_100a"}
+
+
 def _cpu_count():
     try:
         return len(os.sched_getaffinity(0))
@@ -617,6 +655,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
     ap.add_argument("--no-ntt-sweep", action="store_true", help="skip the raw transform sweep")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference CUDA path")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
                     help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
@@ -667,6 +706,9 @@ def main():
             cpu = {"value": round(v, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
                    "sample": f"{ops} ops ({args.cpu_ops} per process x {workers} processes), {busy:.1f} s"}
         per_op = 1e3 / res["per_op_ms"]
+        ref_gpu = None if args.no_reference_gpu else reference_gpu_per_op()
+        if ref_gpu and "value" in ref_gpu:
+            ref_gpu["batched_over_reference_gpu_per_op"] = round(value / (ref_gpu["value"] * world), 2)
         serving = None if args.no_serving else run_serving()
         uneven = None if args.no_uneven else run_uneven()
         sweep = None if args.no_ntt_sweep else run_ntt_sweep()
@@ -685,6 +727,7 @@ def main():
                 "plain_per_op": {"value": round(per_op * world, 2), "unit": "ops/s", "pairs": res["per_op_pairs"],
                                  "form": "one pair per call chain (batch 1), same kernels and keys",
                                  "batched_over_per_op": round(value / (per_op * world), 2)},
+                "reference_gpu_per_op": ref_gpu,
                 "serving": serving,
                 "uneven_batch": uneven,
                 "ntt_sweep": sweep,

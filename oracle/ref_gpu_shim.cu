@@ -1,0 +1,91 @@
+// Test/benchmark infrastructure, not part of the library: times the reference's own
+// CUDA evaluator (troyn:: classes of src/troy_cuda.cuh, compiled from the reference
+// sources by `make -C oracle ref_gpu`) on the batched CKKS workload one ciphertext
+// pair per call — multiply, relinearizeInplace, rescaleToNextInplace,
+// rotateVectorInplace — the "plain per-op GPU path" the batched library is compared
+// with. The decrypted result of the last op is checked against the FP64 product.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <random>
+#include <vector>
+
+#include "troy_cuda.cuh"
+
+using namespace troyn;
+
+extern "C" int ref_gpu_ckks_chain(size_t n, const uint64_t *moduli, int count, int scale_bits, int ops,
+                                  const int *steps, int nsteps, double *ms_per_op, double *max_err) {
+    try {
+        KernelProvider::initialize();
+        EncryptionParameters parms(SchemeType::ckks);
+        parms.setPolyModulusDegree(n);
+        std::vector<Modulus> q;
+        for (int i = 0; i < count; i++) q.emplace_back(moduli[i]);
+        parms.setCoeffModulus(q);
+        SEALContext context(parms, true, SecurityLevel::none);
+        CKKSEncoder encoder(context);
+        KeyGenerator keygen(context);
+        PublicKey pk;
+        keygen.createPublicKey(pk);
+        RelinKeys rlk = keygen.createRelinKeys();
+        GaloisKeys gk = keygen.createGaloisKeys(std::vector<int>(steps, steps + nsteps));
+        Encryptor encryptor(context, pk);
+        Decryptor decryptor(context, keygen.secretKey());
+        Evaluator ev(context);
+        const double scale = std::ldexp(1.0, scale_bits);
+        const size_t slots = n / 2;
+        std::mt19937_64 gen(7);
+        std::uniform_real_distribution<double> u(-1.0, 1.0);
+        std::vector<std::complex<double>> v(slots), w(slots);
+        for (size_t i = 0; i < slots; i++) {
+            v[i] = {u(gen), u(gen)};
+            w[i] = {u(gen), u(gen)};
+        }
+        Plaintext pv, pw;
+        encoder.encode(v, scale, pv);
+        encoder.encode(w, scale, pw);
+        Ciphertext a, b;
+        encryptor.encrypt(pv, a);
+        encryptor.encrypt(pw, b);
+        auto chain = [&](int step, Ciphertext &m) {
+            ev.multiply(a, b, m);
+            ev.relinearizeInplace(m, rlk);
+            ev.rescaleToNextInplace(m);
+            ev.rotateVectorInplace(m, step, gk);
+        };
+        Ciphertext m;
+        for (int i = 0; i < 2; i++) chain(steps[i % nsteps], m);  // warm-up
+        cudaDeviceSynchronize();
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, 0);
+        int last = 0;
+        for (int i = 0; i < ops; i++) {
+            last = steps[i % nsteps];
+            chain(last, m);
+        }
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms_per_op = ms / ops;
+        Plaintext p;
+        decryptor.decrypt(m, p);
+        std::vector<std::complex<double>> got;
+        encoder.decode(p, got);
+        double err = 0;
+        for (size_t i = 0; i < slots; i++) {
+            const size_t j = (i + (size_t)last) % slots;
+            err = std::max(err, std::abs(got[i] - v[j] * w[j]));
+        }
+        *max_err = err;
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    } catch (...) {
+        return 1;
+    }
+}
