@@ -271,11 +271,7 @@ def run_b200(args, rank, world):
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
 
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms, e2e_ms, per_op_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, per_op_ms = float(t[0]), float(t[1]), float(t[2])
+    ms, e2e_ms, per_op_ms = max_over_ranks([ms, e2e_ms, per_op_ms], world, "cuda")
     return {"tuned": tuned,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
@@ -482,6 +478,23 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
     return {"workload": "bfv_n8192_L4_matmul_poisson", "slots": 3, "memory_budget_gb": 16,
             "request_shapes": "in {64..1024} x out {16..256}, MatmulHelper coefficient encoding",
             "latency": "arrival to completion, host steady clock", "runs": runs}
+
+
+def max_over_ranks(times_ms, world, device):
+    """Each timing (ms) maxed over the ranks of the process group (identity for one
+    rank): replicas run independently and the job is as slow as its slowest rank."""
+    if world == 1:
+        return list(times_ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(times_ms), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return units_per_rank * world / (ms * 1e-3)
 
 
 class tb_capi_trace_entry(ctypes.Structure):
@@ -695,8 +708,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_b200(args, rank, world)
     ops_total = PAIRS * world
-    value = ops_total / (res["ms"] * 1e-3)
-    e2e = ops_total / (res["e2e_ms"] * 1e-3)
+    value = job_rate(PAIRS, world, res["ms"])
+    e2e = job_rate(PAIRS, world, res["e2e_ms"])
     line = None
     if rank == 0:
         cpu = None
