@@ -421,7 +421,7 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
     ctx = pytroy.SEALContext(p)
     keygen = pytroy.KeyGenerator(ctx)
     enc = pytroy.BatchEncoder(ctx)
-    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key(), keygen.secret_key())
     rng = np.random.default_rng(2718)
     pool = []
     for _ in range(pool_size):

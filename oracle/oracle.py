@@ -261,7 +261,7 @@ class RefSession:
         L.ref_ct_get.argtypes = [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p, _c.c_void_p]
         L.ref_ct_multiply.argtypes = [_c.c_void_p, _c.c_int, _c.c_int]
         L.ref_ct_add.argtypes = [_c.c_void_p, _c.c_int, _c.c_int]
-        L.ref_ct_encrypt_poly.argtypes = [_c.c_void_p, _u64, _sz]
+        L.ref_ct_encrypt_poly.argtypes = [_c.c_void_p, _u64, _sz, _c.c_int]
         L.ref_ct_multiply_plain_poly.argtypes = [_c.c_void_p, _c.c_int, _u64, _sz]
         L.ref_ct_relinearize.argtypes = [_c.c_void_p, _c.c_int]
         L.ref_ct_rotate.argtypes = [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int]
@@ -369,10 +369,11 @@ class RefSession:
     def mod_switch(self, a):
         return self._check(self.lib.ref_ct_mod_switch(self.h, a))
 
-    def encrypt_poly(self, coeffs):
-        """Encryption of the coefficient-encoded plaintext (encodePolynomial)."""
+    def encrypt_poly(self, coeffs, symmetric=False):
+        """Encryption of the coefficient-encoded plaintext (encodePolynomial), with the
+        public key or (symmetric) the secret key."""
         c = _arr(coeffs)
-        return self._check(self.lib.ref_ct_encrypt_poly(self.h, c, c.size))
+        return self._check(self.lib.ref_ct_encrypt_poly(self.h, c, c.size, int(bool(symmetric))))
 
     def multiply_plain_poly(self, a, coeffs):
         c = _arr(coeffs)

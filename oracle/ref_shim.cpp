@@ -279,7 +279,7 @@ void *ref_session_new(int scheme, size_t n, const uint64_t *moduli, int count, u
         s->context.reset(new SEALContext(*s->parms, true, SecurityLevel::none));
         s->keygen.reset(new KeyGenerator(*s->context));
         s->keygen->createPublicKey(s->pk);
-        s->encryptor.reset(new Encryptor(*s->context, s->pk));
+        s->encryptor.reset(new Encryptor(*s->context, s->pk, s->keygen->secretKey()));
         s->decryptor.reset(new Decryptor(*s->context, s->keygen->secretKey()));
         s->evaluator.reset(new Evaluator(*s->context));
         if (scheme == 2) s->ckks.reset(new CKKSEncoder(*s->context));
@@ -490,13 +490,17 @@ static Plaintext poly_plain(Session *s, const uint64_t *coeffs, size_t count) {
     return p;
 }
 
-// Encrypts BatchEncoder::encodePolynomial(coeffs) (coefficient encoding).
-int ref_ct_encrypt_poly(void *h, const uint64_t *coeffs, size_t count) {
+// Encrypts BatchEncoder::encodePolynomial(coeffs) (coefficient encoding) with the
+// public key, or with the secret key (encryptSymmetric) when symmetric is non-zero.
+int ref_ct_encrypt_poly(void *h, const uint64_t *coeffs, size_t count, int symmetric) {
     auto *s = static_cast<Session *>(h);
     try {
         Plaintext p = poly_plain(s, coeffs, count);
         Ciphertext c;
-        s->encryptor->encrypt(p, c);
+        if (symmetric)
+            s->encryptor->encryptSymmetric(p, c);
+        else
+            s->encryptor->encrypt(p, c);
         return add_ct(s, std::move(c));
     } catch (...) {
         return -1;

@@ -37,6 +37,9 @@ py::array_t<T> to_array(const vector<T> &v) {
 }
 
 using U64Array = py::array_t<uint64_t, py::array::c_style | py::array::forcecast>;
+
+// every element of an array of any shape, row-major
+vector<uint64_t> flat_u64(const U64Array &a) { return vector<uint64_t>(a.data(), a.data() + a.size()); }
 using I64Array = py::array_t<int64_t, py::array::c_style | py::array::forcecast>;
 using F64Array = py::array_t<double, py::array::c_style | py::array::forcecast>;
 using C128Array = py::array_t<complex<double>, py::array::c_style | py::array::forcecast>;
@@ -497,8 +500,43 @@ PYBIND11_MODULE(pytroy, m) {
         .def("complex_conjugate",
              [](const E &self, const C &c, const GK &k) { C r; self.complexConjugate(c, k, r); return r; });
 
-    // MatmulHelper (app/LinearHelper.cuh:197-452; binder.cu:700-760): coefficient-encoded
-    // vector x matrix products, the products of one call fused into one device pass.
+    // Cipher2d / Plain2d (app/LinearHelper.cuh:20-195; binder/binder.cu:700-729). Rows
+    // read as lists (len / indexing) and build from lists of lists as well.
+    using CRows = std::vector<std::vector<Ciphertext>>;
+    using PRows = std::vector<std::vector<Plaintext>>;
+    py::class_<Cipher2d>(m, "Cipher2d")
+        .def(py::init<>())
+        .def(py::init([](CRows rows) {
+            Cipher2d c;
+            c.data = std::move(rows);
+            return c;
+        }))
+        .def("save", [](const Cipher2d &c) { return save_bytes(c); })
+        .def("load", [](Cipher2d &c, const py::bytes &b) { load_bytes(c, b); })
+        .def("load",
+             [](Cipher2d &c, const py::bytes &b, const SEALContext &ctx) {
+                 std::istringstream st{std::string(b)};
+                 c.load(st, ctx);
+             })
+        .def("add_inplace", &Cipher2d::addInplace)
+        .def("add_plain_inplace", &Cipher2d::addPlainInplace)
+        .def("add_plain", &Cipher2d::addPlain)
+        .def("mod_switch_to_next", &Cipher2d::modSwitchToNext)
+        .def("__len__", [](const Cipher2d &c) { return c.data.size(); })
+        .def("__getitem__", [](const Cipher2d &c, std::size_t i) { return c.data.at(i); });
+    py::class_<Plain2d>(m, "Plain2d")
+        .def(py::init<>())
+        .def(py::init([](PRows rows) {
+            Plain2d p;
+            p.data = std::move(rows);
+            return p;
+        }))
+        .def("encrypt", &Plain2d::encrypt)
+        .def("__len__", [](const Plain2d &p) { return p.data.size(); })
+        .def("__getitem__", [](const Plain2d &p, std::size_t i) { return p.data.at(i); });
+
+    // MatmulHelper (app/LinearHelper.cuh:197-530; binder/binder.cu:813-858): coefficient-
+    // encoded matrix products, the products of one call fused into one device pass.
     auto check_len = [](const U64Array &a, std::size_t want, const char *what) {
         if ((std::size_t)a.size() != want) throw std::invalid_argument(std::string(what) + " size incorrect.");
     };
@@ -523,8 +561,72 @@ PYBIND11_MODULE(pytroy, m) {
                  return h.encryptInputs(e, enc, x.data());
              })
         .def("matmul", &MatmulHelper::matmul)
-        .def("decrypt_outputs", [](const MatmulHelper &h, const BatchEncoder &enc, Decryptor &dec, const Cipher2d &c) {
-            return to_array(h.decryptOutputs(enc, dec, c));
+        .def("matmul", &MatmulHelper::matmulCipher)
+        .def("matmul", &MatmulHelper::matmulReverse)
+        .def("encode_outputs",
+             [check_len](const MatmulHelper &h, const BatchEncoder &enc, U64Array y) {
+                 check_len(y, h.plan().batch * h.plan().out, "Output");
+                 return h.encodeOutputs(enc, y.data());
+             })
+        .def("decrypt_outputs",
+             [](const MatmulHelper &h, const BatchEncoder &enc, Decryptor &dec, const Cipher2d &c) {
+                 return to_array(h.decryptOutputs(enc, dec, c));
+             })
+        .def("serialize_outputs",
+             [](const MatmulHelper &h, const Evaluator &ev, const Cipher2d &x) {
+                 std::ostringstream st;
+                 h.serializeOutputs(ev, x, st);
+                 return py::bytes(st.str());
+             })
+        .def("deserialize_outputs",
+             [](const MatmulHelper &h, const Evaluator &ev, const py::bytes &b) {
+                 std::istringstream st{std::string(b)};
+                 return h.deserializeOutputs(ev, st);
+             })
+        .def("serialize_encoded_weights",
+             [](const MatmulHelper &h, const Plain2d &w) {
+                 std::ostringstream st;
+                 h.serializeEncodedWeights(w, st);
+                 return py::bytes(st.str());
+             })
+        .def("deserialize_encoded_weights", [](const MatmulHelper &h, const py::bytes &b) {
+            std::istringstream st{std::string(b)};
+            return h.deserializeEncodedWeights(st);
+        });
+
+    // Conv2dHelper (app/LinearHelper.cuh:531-975; binder/binder.cu:860-896).
+    py::class_<Conv2dHelper>(m, "Conv2dHelper")
+        .def(py::init<std::size_t, std::size_t, std::size_t, std::size_t, std::size_t, std::size_t, std::size_t,
+                      std::size_t>())
+        .def("total_batch_size", &Conv2dHelper::totalBatchSize)
+        .def("encode_weights",
+             [](const Conv2dHelper &h, const BatchEncoder &enc, U64Array w) { return h.encodeWeights(enc, flat_u64(w)); })
+        .def("encode_inputs",
+             [](const Conv2dHelper &h, const BatchEncoder &enc, U64Array x) { return h.encodeInputs(enc, flat_u64(x)); })
+        .def("encrypt_inputs",
+             [](const Conv2dHelper &h, const Encryptor &e, const BatchEncoder &enc, U64Array x) {
+                 return h.encryptInputs(e, enc, flat_u64(x));
+             })
+        .def("conv2d", &Conv2dHelper::conv2d)
+        .def("conv2d", &Conv2dHelper::conv2dCipher)
+        .def("conv2d", &Conv2dHelper::conv2dReverse)
+        .def("encode_outputs",
+             [](const Conv2dHelper &h, const BatchEncoder &enc, U64Array y) { return h.encodeOutputs(enc, flat_u64(y)); })
+        .def("add_plain_inplace", &Conv2dHelper::addPlainInplace)
+        .def("add_inplace", &Conv2dHelper::addInplace)
+        .def("decrypt_outputs",
+             [](const Conv2dHelper &h, const BatchEncoder &enc, Decryptor &dec, const Cipher2d &c) {
+                 return to_array(h.decryptOutputs(enc, dec, c));
+             })
+        .def("serialize_outputs",
+             [](const Conv2dHelper &h, const Evaluator &ev, const Cipher2d &x) {
+                 std::ostringstream st;
+                 h.serializeOutputs(ev, x, st);
+                 return py::bytes(st.str());
+             })
+        .def("deserialize_outputs", [](const Conv2dHelper &h, const Evaluator &ev, const py::bytes &b) {
+            std::istringstream st{std::string(b)};
+            return h.deserializeOutputs(ev, st);
         });
 
     // Continuous-batching server of single-row MatmulHelper products.

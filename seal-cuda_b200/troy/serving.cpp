@@ -1,5 +1,4 @@
-// MatmulHelper (app/LinearHelper.cuh:197-452) and the continuous-batching
-// MatmulServer over the library's batched device operations.
+// The continuous-batching MatmulServer over the library's batched device operations.
 #include "serving.hpp"
 
 #include <cuda_runtime_api.h>
@@ -13,26 +12,8 @@ namespace troyn {
 
 namespace {
 
-std::size_t ceil_div(std::size_t a, std::size_t b) { return (a + b - 1) / b; }
-
 void cuda_ok(cudaError_t e, const char *what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-void tb_ok(int st) {
-    if (st == TB_OK) return;
-    if (st == TB_ERR_INVALID_ARGUMENT) throw std::invalid_argument(tb_last_error());
-    if (st == TB_ERR_UNSUPPORTED) throw std::logic_error(tb_last_error());
-    throw std::runtime_error(tb_last_error());
-}
-
-// uint32 arrays travel packed two per device word.
-DeviceBuffer upload_u32(const std::vector<uint32_t> &v) {
-    std::vector<uint64_t> w((v.size() + 1) / 2, 0);
-    if (!v.empty()) std::memcpy(w.data(), v.data(), v.size() * 4);
-    DeviceBuffer b;
-    b.fromHost(w.data(), w.size());
-    return b;
 }
 
 // Record of tb_matmul_encode_weights: {offset lo, offset hi, in, out, ib, ob, li, lj}.
@@ -48,184 +29,6 @@ void push_block(std::vector<uint32_t> &d, uint64_t src, const MatmulPlan &p, std
 }
 
 }  // namespace
-
-// ------------------------------------------------------------------ plan
-
-MatmulPlan MatmulPlan::make(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots) {
-    if (!batch || !in || !out || !slots) throw std::invalid_argument("matmul dimensions must be positive");
-    MatmulPlan p;
-    p.batch = batch;
-    p.in = in;
-    p.out = out;
-    p.slots = slots;
-    std::size_t best = 2147483647;
-    for (std::size_t b = batch; b >= 1; b--) {
-        const std::size_t bc = ceil_div(batch, b);
-        if (b >= slots) continue;
-        if (bc * 2 > best) continue;
-        for (std::size_t i = 1; i < slots / b; i++) {
-            std::size_t o = std::min(slots / b / i, out);
-            if (i > in || o < 1) continue;
-            const std::size_t c = bc * (ceil_div(in, i) + ceil_div(out, o));
-            if (c >= best) continue;
-            p.batchBlock = b;
-            p.inputBlock = i;
-            p.outputBlock = o;
-            best = c;
-        }
-    }
-    if (!p.batchBlock) throw std::invalid_argument("matmul shape does not fit the slot count");
-    return p;
-}
-
-// ------------------------------------------------------------------ helper
-
-Plain2d MatmulHelper::encodeWeights(const BatchEncoder &encoder, const uint64_t *weights) const {
-    const auto &p = plan_;
-    Plain2d out;
-    for (std::size_t li = 0; li < p.in; li += p.inputBlock) {
-        const std::size_t ui = std::min(li + p.inputBlock, p.in);
-        std::vector<Plaintext> row;
-        for (std::size_t lj = 0; lj < p.out; lj += p.outputBlock) {
-            const std::size_t uj = std::min(lj + p.outputBlock, p.out);
-            std::vector<uint64_t> vec(p.inputBlock * p.outputBlock, 0);
-            for (std::size_t j = lj; j < uj; j++)
-                for (std::size_t i = li; i < ui; i++)
-                    vec[(j - lj) * p.inputBlock + p.inputBlock - (i - li) - 1] = weights[i * p.out + j];
-            Plaintext pt;
-            encoder.encodePolynomial(vec, pt);
-            row.push_back(std::move(pt));
-        }
-        out.push_back(std::move(row));
-    }
-    return out;
-}
-
-Plain2d MatmulHelper::encodeInputs(const BatchEncoder &encoder, const uint64_t *inputs) const {
-    const auto &p = plan_;
-    Plain2d out;
-    for (std::size_t li = 0; li < p.batch; li += p.batchBlock) {
-        const std::size_t ui = std::min(li + p.batchBlock, p.batch);
-        std::vector<Plaintext> row;
-        for (std::size_t lj = 0; lj < p.in; lj += p.inputBlock) {
-            const std::size_t uj = std::min(lj + p.inputBlock, p.in);
-            std::vector<uint64_t> vec(p.slots, 0);
-            for (std::size_t i = li; i < ui; i++)
-                for (std::size_t j = lj; j < uj; j++)
-                    vec[(i - li) * p.inputBlock * p.outputBlock + (j - lj)] = inputs[i * p.in + j];
-            Plaintext pt;
-            encoder.encodePolynomial(vec, pt);
-            row.push_back(std::move(pt));
-        }
-        out.push_back(std::move(row));
-    }
-    return out;
-}
-
-Cipher2d MatmulHelper::encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder,
-                                     const uint64_t *inputs) const {
-    Cipher2d out;
-    for (auto &row : encodeInputs(encoder, inputs)) {
-        std::vector<Ciphertext> r;
-        for (auto &pt : row) {
-            Ciphertext c;
-            encryptor.encrypt(pt, c);
-            r.push_back(std::move(c));
-        }
-        out.push_back(std::move(r));
-    }
-    return out;
-}
-
-// MatmulHelper::matmul (app/LinearHelper.cuh:323-346) as one pass: every input
-// transformed once, every weight lifted and transformed once, each output the sum of
-// its products accumulated in one kernel, one inverse transform per output.
-Cipher2d MatmulHelper::matmul(const Evaluator &ev, const Cipher2d &a, const Plain2d &w) const {
-    const auto &p = plan_;
-    const SEALContext &ctx = ev.context();
-    if (ctx.scheme() != SchemeType::bfv && ctx.scheme() != SchemeType::bgv) throw std::logic_error("unsupported scheme");
-    if (a.size() != p.batchBlocks()) throw std::invalid_argument("Input batchsize incorrect.");
-    if (w.size() != p.inputBlocks()) throw std::invalid_argument("Weight input dimension incorrect.");
-    const std::size_t nb = p.batchBlocks(), ni = p.inputBlocks(), no = p.outputBlocks(), n = ctx.polyModulusDegree();
-    const Ciphertext &first = a.at(0).at(0);
-    auto d = ctx.getContextData(first.parmsID());
-    if (!d) throw std::invalid_argument("encrypted is not valid for encryption parameters");
-    const int L = d->levelLimbs();
-    const std::size_t ctw = 2 * (std::size_t)L * n, ptw = (std::size_t)L * n;
-    DeviceBuffer A(nb * ni * ctw), Wr(ni * no * n), Wn(ni * no * ptw), O(nb * no * ctw);
-    for (std::size_t b = 0; b < nb; b++) {
-        if (a[b].size() != ni) throw std::invalid_argument("Input dimension incorrect.");
-        for (std::size_t i = 0; i < ni; i++) {
-            const Ciphertext &c = a[b][i];
-            if (c.parmsID() != first.parmsID() || c.size() != 2 || c.isNttForm() ||
-                c.correctionFactor() != first.correctionFactor())
-                throw std::invalid_argument("inputs must be size-2 ciphertexts of one level and correction factor");
-            cuda_ok(cudaMemcpyAsync(A.get() + (b * ni + i) * ctw, c.data(), ctw * 8, cudaMemcpyDeviceToDevice, 0),
-                    "device copy");
-        }
-    }
-    Wr.zero();
-    for (std::size_t i = 0; i < ni; i++) {
-        if (w[i].size() != no) throw std::invalid_argument("Weight output dimension incorrect.");
-        for (std::size_t j = 0; j < no; j++) {
-            const Plaintext &pt = w[i][j];
-            if (pt.isNttForm() || pt.coeffCount() > n) throw std::invalid_argument("weights must be coefficient plaintexts");
-            if (pt.coeffCount())
-                cuda_ok(cudaMemcpyAsync(Wr.get() + (i * no + j) * n, pt.data(), pt.coeffCount() * 8,
-                                        cudaMemcpyDeviceToDevice, 0),
-                        "device copy");
-        }
-    }
-    std::vector<uint32_t> off{0}, ia, iw;
-    for (std::size_t b = 0; b < nb; b++)
-        for (std::size_t j = 0; j < no; j++) {
-            for (std::size_t i = 0; i < ni; i++) {
-                ia.push_back((uint32_t)(b * ni + i));
-                iw.push_back((uint32_t)(i * no + j));
-            }
-            off.push_back((uint32_t)ia.size());
-        }
-    DeviceBuffer doff = upload_u32(off), dia = upload_u32(ia), diw = upload_u32(iw);
-    tb_context *h = ctx.handle();
-    tb_ok(tb_ntt_forward(h, A.get(), A.get(), 2 * nb * ni, 0, L, 0, nullptr));
-    tb_ok(tb_plain_to_ntt(h, L, Wr.get(), n, n, Wn.get(), ni * no, nullptr));
-    tb_ok(tb_dyadic_accumulate(h, L, 2, A.get(), 0, Wn.get(), 0, O.get(), 0, (const uint32_t *)doff.get(),
-                               (const uint32_t *)dia.get(), (const uint32_t *)diw.get(), (uint32_t)(nb * no), nullptr));
-    tb_ok(tb_ntt_inverse(h, O.get(), O.get(), 2 * nb * no, 0, L, 0, nullptr));
-    Cipher2d out(nb);
-    for (std::size_t b = 0; b < nb; b++)
-        for (std::size_t j = 0; j < no; j++) {
-            Ciphertext c(ctx, first.parmsID(), 2);
-            cuda_ok(cudaMemcpyAsync(c.data(), O.get() + (b * no + j) * ctw, ctw * 8, cudaMemcpyDeviceToDevice, 0),
-                    "device copy");
-            c.correctionFactor() = first.correctionFactor();
-            out[b].push_back(std::move(c));
-        }
-    return out;
-}
-
-std::vector<uint64_t> MatmulHelper::decryptOutputs(const BatchEncoder &encoder, Decryptor &decryptor,
-                                                   const Cipher2d &outputs) const {
-    const auto &p = plan_;
-    std::vector<uint64_t> dec(p.batch * p.out);
-    std::size_t di = 0;
-    for (std::size_t li = 0; li < p.batch; li += p.batchBlock, di++) {
-        const std::size_t ui = std::min(li + p.batchBlock, p.batch);
-        std::size_t dj = 0;
-        for (std::size_t lj = 0; lj < p.out; lj += p.outputBlock, dj++) {
-            const std::size_t uj = std::min(lj + p.outputBlock, p.out);
-            Plaintext pt;
-            decryptor.decrypt(outputs.at(di).at(dj), pt);
-            std::vector<uint64_t> buf;
-            encoder.decodePolynomial(pt, buf);
-            for (std::size_t i = li; i < ui; i++)
-                for (std::size_t j = lj; j < uj; j++)
-                    dec[i * p.out + j] =
-                        buf[(i - li) * p.inputBlock * p.outputBlock + (j - lj) * p.inputBlock + p.inputBlock - 1];
-        }
-    }
-    return dec;
-}
 
 // ------------------------------------------------------------------ server
 

@@ -1,11 +1,5 @@
-// Encrypted vector x plaintext-matrix products (the reference's app/LinearHelper.cuh
-// MatmulHelper, coefficient encoding) and a continuous-batching server for them.
-//
-// MatmulHelper keeps the reference's block planning and encodings; its matmul runs
-// every product of a call in one pass on the device (inputs transformed once,
-// weights lifted and transformed once, all sums of products accumulated in one
-// kernel, one inverse transform per output) instead of one multiplyPlain and
-// addInplace per block pair. The sums are exact, so outputs are word-identical.
+// A continuous-batching server for encrypted vector x plaintext-matrix products
+// (MatmulHelper's coefficient encoding, app/LinearHelper.cuh).
 //
 // MatmulServer serves a stream of single-row requests of different shapes: requests
 // wait in a FIFO queue; whenever one of its `slots` streams is free it admits queued
@@ -23,40 +17,9 @@
 #include <memory>
 #include <vector>
 
-#include "troy_b200.hpp"
+#include "linear.hpp"
 
 namespace troyn {
-
-// Block shape of MatmulHelper::determineBlock (app/LinearHelper.cuh:206-228).
-struct MatmulPlan {
-    std::size_t batch = 0, in = 0, out = 0, slots = 0;
-    std::size_t batchBlock = 0, inputBlock = 0, outputBlock = 0;
-    static MatmulPlan make(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots);
-    std::size_t batchBlocks() const { return (batch + batchBlock - 1) / batchBlock; }
-    std::size_t inputBlocks() const { return (in + inputBlock - 1) / inputBlock; }
-    std::size_t outputBlocks() const { return (out + outputBlock - 1) / outputBlock; }
-};
-
-using Plain2d = std::vector<std::vector<Plaintext>>;
-using Cipher2d = std::vector<std::vector<Ciphertext>>;
-
-class MatmulHelper {
-public:
-    MatmulHelper(std::size_t batch, std::size_t in, std::size_t out, std::size_t slots)
-        : plan_(MatmulPlan::make(batch, in, out, slots)) {}
-    const MatmulPlan &plan() const { return plan_; }
-    // encodeWeights / encodeInputs / encryptInputs / decryptOutputs
-    // (app/LinearHelper.cuh:258-452): coefficient encodings of the reference.
-    Plain2d encodeWeights(const BatchEncoder &encoder, const std::uint64_t *weights) const;
-    Plain2d encodeInputs(const BatchEncoder &encoder, const std::uint64_t *inputs) const;
-    Cipher2d encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder, const std::uint64_t *inputs) const;
-    Cipher2d matmul(const Evaluator &evaluator, const Cipher2d &a, const Plain2d &w) const;
-    std::vector<std::uint64_t> decryptOutputs(const BatchEncoder &encoder, Decryptor &decryptor,
-                                              const Cipher2d &outputs) const;
-
-private:
-    MatmulPlan plan_;
-};
 
 class MatmulServer {
 public:

@@ -51,7 +51,7 @@ def test_matmul_helper_matches_reference_cpu_words():
     ctx, t = _context(seeded=True)
     keygen = pytroy.KeyGenerator(ctx)
     enc = pytroy.BatchEncoder(ctx)
-    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key(), keygen.secret_key())
     ev = pytroy.Evaluator(ctx)
     inp, out = 300, 40
     h = pytroy.MatmulHelper(1, inp, out, N)
@@ -68,7 +68,7 @@ def test_matmul_helper_matches_reference_cpu_words():
         vec = np.zeros(N, np.uint64)
         seg = x[bi * ib:(bi + 1) * ib]
         vec[:seg.size] = seg
-        ids.append(ref.encrypt_poly(vec))
+        ids.append(ref.encrypt_poly(vec, symmetric=True))  # Plain2d::encrypt is symmetric
         assert np.array_equal(ref.ct(ids[-1])["data"].reshape(-1), np.asarray(cts[0][bi].data(), np.uint64))
     W = w.reshape(inp, out)
     for bj in range(no):
@@ -92,7 +92,7 @@ def serving():
     ns = type("NS", (), {})()
     ns.ctx, ns.t = ctx, t
     ns.enc = pytroy.BatchEncoder(ctx)
-    ns.encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    ns.encryptor = pytroy.Encryptor(ctx, keygen.create_public_key(), keygen.secret_key())
     ns.dec = pytroy.Decryptor(ctx, keygen.secret_key())
     ns.ev = pytroy.Evaluator(ctx)
     rng = np.random.default_rng(29)
@@ -177,7 +177,7 @@ def test_server_results_identical_alone_and_in_the_mix(serving):
             c = pytroy.Ciphertext()
             c.load(_ct_bytes(ns.ctx, alone[k][j * per:(j + 1) * per]), ns.ctx)
             outs.append(c)
-        assert np.array_equal(h.decrypt_outputs(ns.enc, ns.dec, [outs]), _expected(x, w, ns.t, inp, out)), k
+        assert np.array_equal(h.decrypt_outputs(ns.enc, ns.dec, pytroy.Cipher2d([outs])), _expected(x, w, ns.t, inp, out)), k
 
 
 def test_admission_by_memory_footprint(serving):
