@@ -4,6 +4,8 @@ Conv2dHelper. Each function returns the coefficient vectors that the reference f
 to BatchEncoder::encodePolynomial, so the reference's own CPU evaluator
 (oracle.RefSession) can encrypt and multiply the same polynomials, and
 `negacyclic_mul` lets the layouts be checked against a direct product on the CPU."""
+import math
+
 import numpy as np
 
 
@@ -169,3 +171,60 @@ def negacyclic_mul(a, b, n, t):
     res = full[:n].copy()
     res[:len(full) - n] -= full[n:]
     return (res % t).astype(np.uint64)
+
+
+def next_pow2(v):
+    """nextPow2 (app/matmul.cuh:15): 2^ceil(log(v) / log(2)) in double precision."""
+    return int(2.0 ** math.ceil(math.log(v) / math.log(2.0)))
+
+
+class DiagonalLayout:
+    """Slot layout of the diagonal CKKS matrix-vector product (app/matmul.cuh:5-123)."""
+
+    def __init__(self, height, width, slots):
+        self.height, self.width, self.slots = height, width, slots
+        self.p2 = next_pow2(width)
+        self.pack = slots // self.p2
+        self.count = int(math.ceil(np.float32(next_pow2(height)) / np.float32(self.pack)))
+
+    def input(self, v):
+        """prepareInput (app/matmul.cuh:19-32): v repeated pack times, p2 slots apart."""
+        out = np.zeros(self.slots, np.complex128)
+        for idx in range(self.pack):
+            out[idx * self.p2:idx * self.p2 + self.width] = v
+        return out
+
+    def diagonals(self, m):
+        """encode (app/matmul.cuh:45-90): rows packed count at a time, then repacked
+        into generalized diagonals."""
+        m = np.asarray(m, np.complex128)
+        pack = np.zeros((self.count, self.slots), np.complex128)
+        for row in range(self.height):
+            c = row // self.count
+            pack[row % self.count, c * self.p2:c * self.p2 + self.width] = m[row]
+        mod_mask, wrap_mask = self.count - 1, self.p2 - 1
+        diag = np.zeros_like(pack)
+        for ct in range(self.count):
+            for col in range(self.slots):
+                dl = (col - ct) & wrap_mask & mod_mask
+                dh = (col ^ ct) & self.slots & mod_mask
+                cl = (col - dl) & wrap_mask
+                ch = (self.p2 * (col // self.p2)) ^ dh
+                diag[dh + dl, ch + cl] = pack[ct, col]
+        return diag
+
+    def rows(self, slots):
+        """decodeResult (app/matmul.cuh:34-43)."""
+        return np.array([slots[(i % self.count) + self.p2 * (i // self.count)] for i in range(self.height)])
+
+    def apply(self, m, v):
+        """The product on plain slot vectors: sum_i rotate(x, i) * diag_i, then the
+        rotate-and-add folds (rotate by k: slot j takes slot j + k)."""
+        x = self.input(v)
+        d = self.diagonals(m)
+        r = sum(np.roll(x, -i) * d[i] for i in range(self.count))
+        rot = self.count
+        while rot < self.p2:
+            r = r + np.roll(r, -rot)
+            rot *= 2
+        return self.rows(r)

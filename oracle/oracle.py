@@ -263,6 +263,9 @@ class RefSession:
         L.ref_ct_add.argtypes = [_c.c_void_p, _c.c_int, _c.c_int]
         L.ref_ct_encrypt_poly.argtypes = [_c.c_void_p, _u64, _sz, _c.c_int]
         L.ref_ct_multiply_plain_poly.argtypes = [_c.c_void_p, _c.c_int, _u64, _sz]
+        L.ref_ct_from_words.argtypes = [_c.c_void_p, _u64, _sz, _sz, _c.c_int, _c.c_double, _c.c_uint64]
+        L.ref_ct_encrypt_plain_words.argtypes = [_c.c_void_p, _u64, _sz, _c.c_double, _c.c_int]
+        L.ref_ct_multiply_plain_words.argtypes = [_c.c_void_p, _c.c_int, _u64, _sz, _c.c_double]
         L.ref_ct_relinearize.argtypes = [_c.c_void_p, _c.c_int]
         L.ref_ct_rotate.argtypes = [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int]
         L.ref_ct_rescale.argtypes = [_c.c_void_p, _c.c_int]
@@ -378,6 +381,21 @@ class RefSession:
     def multiply_plain_poly(self, a, coeffs):
         c = _arr(coeffs)
         return self._check(self.lib.ref_ct_multiply_plain_poly(self.h, a, c, c.size))
+
+    def ct_from_words(self, words, size, limbs, ntt, scale=1.0, correction=1):
+        """A ciphertext given as words (size x limbs x n) at the level with `limbs` primes."""
+        w = _arr(words)
+        return self._check(self.lib.ref_ct_from_words(self.h, w, size, limbs, int(bool(ntt)), scale, correction))
+
+    def encrypt_plain_words(self, words, scale=1.0, symmetric=False):
+        """Encryption of a plaintext given as words at the first level (CKKS: NTT form)."""
+        w = _arr(words)
+        return self._check(self.lib.ref_ct_encrypt_plain_words(self.h, w, w.size, scale, int(bool(symmetric))))
+
+    def multiply_plain_words(self, a, words, scale=1.0):
+        """multiplyPlain by a plaintext given as words at the ciphertext's level."""
+        w = _arr(words)
+        return self._check(self.lib.ref_ct_multiply_plain_words(self.h, a, w, w.size, scale))
 
     def multiply_plain_slots(self, a, slots):
         s = _arr(slots)

@@ -520,6 +520,65 @@ int ref_ct_multiply_plain_poly(void *h, int a, const uint64_t *coeffs, size_t co
     }
 }
 
+// A plaintext given as words at parms_id (NTT-form CKKS plaintexts carry L*N words).
+static Plaintext words_plain(Session *s, const ParmsID &id, const uint64_t *words, size_t count, double scale) {
+    Plaintext p;
+    p.resize(count);
+    std::memcpy(p.data(), words, count * 8);
+    if (s->scheme == SchemeType::ckks) p.parmsID() = id;
+    p.scale() = scale;
+    return p;
+}
+
+// A ciphertext given as words: `size` polynomials at the level with `limbs` primes.
+int ref_ct_from_words(void *h, const uint64_t *words, size_t size, size_t limbs, int is_ntt, double scale,
+                      uint64_t corr) {
+    auto *s = static_cast<Session *>(h);
+    try {
+        auto cd = s->context->firstContextData();
+        while (cd && cd->parms().coeffModulus().size() != limbs) cd = cd->nextContextData();
+        if (!cd) return -1;
+        Ciphertext c;
+        c.resize(*s->context, cd->parmsID(), size);
+        std::memcpy(c.data(), words, size * limbs * s->parms->polyModulusDegree() * 8);
+        c.isNttForm() = is_ntt != 0;
+        c.scale() = scale;
+        c.correctionFactor() = corr;
+        return add_ct(s, std::move(c));
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Encrypts a plaintext given as words at the first level.
+int ref_ct_encrypt_plain_words(void *h, const uint64_t *words, size_t count, double scale, int symmetric) {
+    auto *s = static_cast<Session *>(h);
+    try {
+        Plaintext p = words_plain(s, s->context->firstParmsID(), words, count, scale);
+        Ciphertext c;
+        if (symmetric)
+            s->encryptor->encryptSymmetric(p, c);
+        else
+            s->encryptor->encrypt(p, c);
+        return add_ct(s, std::move(c));
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Evaluator::multiplyPlain by a plaintext given as words at the ciphertext's level.
+int ref_ct_multiply_plain_words(void *h, int a, const uint64_t *words, size_t count, double scale) {
+    auto *s = static_cast<Session *>(h);
+    try {
+        Plaintext p = words_plain(s, s->cts.at(a).parmsID(), words, count, scale);
+        Ciphertext c;
+        s->evaluator->multiplyPlain(s->cts.at(a), p, c);
+        return add_ct(s, std::move(c));
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_ct_add(void *h, int a, int b) {
     auto *s = static_cast<Session *>(h);
     try {

@@ -12,6 +12,7 @@
 
 #include <sstream>
 
+#include "linear_ckks.hpp"
 #include "serving.hpp"
 #include "troy_b200.hpp"
 
@@ -40,6 +41,9 @@ using U64Array = py::array_t<uint64_t, py::array::c_style | py::array::forcecast
 
 // every element of an array of any shape, row-major
 vector<uint64_t> flat_u64(const U64Array &a) { return vector<uint64_t>(a.data(), a.data() + a.size()); }
+vector<double> flat_f64(const py::array_t<double, py::array::c_style | py::array::forcecast> &a) {
+    return vector<double>(a.data(), a.data() + a.size());
+}
 using I64Array = py::array_t<int64_t, py::array::c_style | py::array::forcecast>;
 using F64Array = py::array_t<double, py::array::c_style | py::array::forcecast>;
 using C128Array = py::array_t<complex<double>, py::array::c_style | py::array::forcecast>;
@@ -628,6 +632,105 @@ PYBIND11_MODULE(pytroy, m) {
             std::istringstream st{std::string(b)};
             return h.deserializeOutputs(ev, st);
         });
+
+    // LinearHelperCKKS (app/LinearHelperCKKS.cuh), bound with the method names of the
+    // reference binder's CKKS helper bindings (binder/binder.cu:731-811).
+    using F64 = py::array_t<double, py::array::c_style | py::array::forcecast>;
+    py::class_<LinearHelperCKKS::MatmulHelper>(m, "CkksMatmulHelper")
+        .def(py::init<std::size_t, std::size_t, std::size_t, std::size_t>())
+        .def_property_readonly("block_height", &LinearHelperCKKS::MatmulHelper::blockHeight)
+        .def_property_readonly("block_width", &LinearHelperCKKS::MatmulHelper::blockWidth)
+        .def_readwrite("encoded_weights", &LinearHelperCKKS::MatmulHelper::encodedWeights)
+        .def("encode_weights",
+             [](LinearHelperCKKS::MatmulHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 w, double scale) {
+                 h.encodeWeights(enc, id, flat_f64(w), scale);
+             })
+        .def("encode_inputs",
+             [](const LinearHelperCKKS::MatmulHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 x,
+                double scale) { return h.encodeInputs(enc, id, flat_f64(x), scale); })
+        .def("encrypt_inputs",
+             [](const LinearHelperCKKS::MatmulHelper &h, const Encryptor &e, const CKKSEncoder &enc, const ParmsID &id,
+                F64 x, double scale) { return h.encryptInputs(e, enc, id, flat_f64(x), scale); })
+        .def("matmul", &LinearHelperCKKS::MatmulHelper::matmul)
+        .def("encode_outputs",
+             [](const LinearHelperCKKS::MatmulHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 y,
+                double scale) { return h.encodeOutputs(enc, id, flat_f64(y), scale); })
+        .def("add_plain_inplace", &LinearHelperCKKS::MatmulHelper::addPlainInplace)
+        .def("decrypt_outputs",
+             [](const LinearHelperCKKS::MatmulHelper &h, const CKKSEncoder &enc, Decryptor &dec, const Cipher2d &c) {
+                 return to_array(h.decryptOutputs(enc, dec, c));
+             })
+        .def("serialize_outputs",
+             [](const LinearHelperCKKS::MatmulHelper &h, const Evaluator &ev, const Cipher2d &x) {
+                 std::ostringstream st;
+                 h.serializeOutputs(ev, x, st);
+                 return py::bytes(st.str());
+             })
+        .def("deserialize_outputs", [](const LinearHelperCKKS::MatmulHelper &h, const Evaluator &ev, const py::bytes &b) {
+            std::istringstream st{std::string(b)};
+            return h.deserializeOutputs(ev, st);
+        });
+    py::class_<LinearHelperCKKS::Conv2dHelper>(m, "CkksConv2dHelper")
+        .def(py::init<std::size_t, std::size_t, std::size_t, std::size_t, std::size_t, std::size_t, std::size_t,
+                      std::size_t>())
+        .def("total_batch_size", &LinearHelperCKKS::Conv2dHelper::totalBatchSize)
+        .def_readwrite("encoded_weights", &LinearHelperCKKS::Conv2dHelper::encodedWeights)
+        .def("encode_weights",
+             [](LinearHelperCKKS::Conv2dHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 w, double scale) {
+                 h.encodeWeights(enc, id, flat_f64(w), scale);
+             })
+        .def("encode_inputs",
+             [](const LinearHelperCKKS::Conv2dHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 x,
+                double scale) { return h.encodeInputs(enc, id, flat_f64(x), scale); })
+        .def("encrypt_inputs",
+             [](const LinearHelperCKKS::Conv2dHelper &h, const Encryptor &e, const CKKSEncoder &enc, const ParmsID &id,
+                F64 x, double scale) { return h.encryptInputs(e, enc, id, flat_f64(x), scale); })
+        .def("conv2d", &LinearHelperCKKS::Conv2dHelper::conv2d)
+        .def("encode_outputs",
+             [](const LinearHelperCKKS::Conv2dHelper &h, const CKKSEncoder &enc, const ParmsID &id, F64 y,
+                double scale) { return h.encodeOutputs(enc, id, flat_f64(y), scale); })
+        .def("add_plain_inplace", &LinearHelperCKKS::Conv2dHelper::addPlainInplace)
+        .def("add_inplace", &LinearHelperCKKS::Conv2dHelper::addInplace)
+        .def("decrypt_outputs",
+             [](const LinearHelperCKKS::Conv2dHelper &h, const CKKSEncoder &enc, Decryptor &dec, const Cipher2d &c) {
+                 return to_array(h.decryptOutputs(enc, dec, c));
+             })
+        .def("serialize_outputs",
+             [](const LinearHelperCKKS::Conv2dHelper &h, const Evaluator &ev, const Cipher2d &x) {
+                 std::ostringstream st;
+                 h.serializeOutputs(ev, x, st);
+                 return py::bytes(st.str());
+             })
+        .def("deserialize_outputs", [](const LinearHelperCKKS::Conv2dHelper &h, const Evaluator &ev, const py::bytes &b) {
+            std::istringstream st{std::string(b)};
+            return h.deserializeOutputs(ev, st);
+        });
+
+    // The diagonal CKKS matrix-vector product (app/matmul.cuh).
+    using C128 = py::array_t<complex<double>, py::array::c_style | py::array::forcecast>;
+    py::class_<DiagonalMatmulHelper>(m, "DiagonalMatmulHelper")
+        .def(py::init<std::size_t, std::size_t, std::size_t>())
+        .def_property_readonly("pack_num", &DiagonalMatmulHelper::packNum)
+        .def_property_readonly("cipher_count", &DiagonalMatmulHelper::cipherCount)
+        .def("prepare_input",
+             [](const DiagonalMatmulHelper &h, C128 x, const CKKSEncoder &enc, double scale) {
+                 return h.prepareInput(vector<complex<double>>(x.data(), x.data() + x.size()), enc, scale);
+             })
+        .def("decode_result",
+             [](const DiagonalMatmulHelper &h, const Plaintext &p, const CKKSEncoder &enc) {
+                 return to_array(h.decodeResult(p, enc));
+             })
+        .def("encode",
+             [](DiagonalMatmulHelper &h, C128 mat, const CKKSEncoder &enc, double scale) {
+                 if (mat.ndim() != 2) throw std::invalid_argument("matrix must be 2-d");
+                 const auto r = mat.unchecked<2>();
+                 vector<vector<complex<double>>> rows(mat.shape(0), vector<complex<double>>(mat.shape(1)));
+                 for (py::ssize_t i = 0; i < mat.shape(0); i++)
+                     for (py::ssize_t j = 0; j < mat.shape(1); j++) rows[i][j] = r(i, j);
+                 h.encode(rows, enc, scale);
+             })
+        .def("multiply", &DiagonalMatmulHelper::multiply, py::arg("repeated_vector"), py::arg("evaluator"),
+             py::arg("galois_keys"), py::arg("rescale"));
 
     // Continuous-batching server of single-row MatmulHelper products.
     py::class_<MatmulServer>(m, "MatmulServer")

@@ -2,6 +2,8 @@
 // library's fused device sum of products.
 #include "linear.hpp"
 
+#include "device_util.hpp"
+
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
@@ -16,18 +18,11 @@ namespace troyn {
 
 namespace {
 
+using detail::cuda_ok;
+using detail::tb_ok;
+using detail::upload_u32;
+
 std::size_t ceil_div(std::size_t a, std::size_t b) { return (a + b - 1) / b; }
-
-void cuda_ok(cudaError_t e, const char *what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-void tb_ok(int st) {
-    if (st == TB_OK) return;
-    if (st == TB_ERR_INVALID_ARGUMENT) throw std::invalid_argument(tb_last_error());
-    if (st == TB_ERR_UNSUPPORTED) throw std::logic_error(tb_last_error());
-    throw std::runtime_error(tb_last_error());
-}
 
 template <class T>
 void put(std::ostream &s, const T &v) {
@@ -40,15 +35,6 @@ T get(std::istream &s) {
     s.read(reinterpret_cast<char *>(&v), sizeof(T));
     if (!s) throw std::invalid_argument("unexpected end of stream");
     return v;
-}
-
-// uint32 arrays travel packed two per device word.
-DeviceBuffer upload_u32(const std::vector<uint32_t> &v) {
-    std::vector<uint64_t> w((v.size() + 1) / 2, 0);
-    if (!v.empty()) std::memcpy(w.data(), v.data(), v.size() * 4);
-    DeviceBuffer b;
-    b.fromHost(w.data(), w.size());
-    return b;
 }
 
 void check_rect(std::size_t a, std::size_t b) {
@@ -134,44 +120,77 @@ std::vector<Ciphertext> sumOfProducts(const Evaluator &ev, const std::vector<con
                                       const std::vector<const Plaintext *> &pts, const std::vector<uint32_t> &off,
                                       const std::vector<uint32_t> &ia, const std::vector<uint32_t> &iw) {
     const SEALContext &ctx = ev.context();
-    if (ctx.scheme() != SchemeType::bfv && ctx.scheme() != SchemeType::bgv) throw std::logic_error("unsupported scheme");
-    if (cts.empty() || off.size() < 2) throw std::invalid_argument("no products");
+    if (cts.empty() || pts.empty() || off.size() < 2) throw std::invalid_argument("no products");
     const Ciphertext &first = *cts[0];
     auto d = ctx.getContextData(first.parmsID());
     if (!d) throw std::invalid_argument("encrypted is not valid for encryption parameters");
     const int L = d->levelLimbs();
-    const std::size_t n = ctx.polyModulusDegree(), ctw = 2 * (std::size_t)L * n, ptw = (std::size_t)L * n;
+    const bool ntt = first.isNttForm();
+    const std::size_t size = first.size();
+    if (size < 2) throw std::invalid_argument("encrypted is empty");
+    if (!ntt && ctx.scheme() != SchemeType::bfv && ctx.scheme() != SchemeType::bgv)
+        throw std::invalid_argument("encrypted must be in NTT form");
+    const std::size_t n = ctx.polyModulusDegree(), ctw = size * (std::size_t)L * n, ptw = (std::size_t)L * n;
     const std::size_t na = cts.size(), np = pts.size(), no = off.size() - 1;
+    if (off[0] != 0 || off[no] != ia.size() || ia.size() != iw.size()) throw std::invalid_argument("bad term lists");
+    for (std::size_t o = 0; o < no; o++)
+        if (off[o + 1] <= off[o]) throw std::invalid_argument("every output needs a product");
     for (std::size_t k = 0; k < ia.size(); k++)
         if (ia[k] >= na || iw[k] >= np) throw std::invalid_argument("product index out of range");
-    DeviceBuffer A(na * ctw), Wr(np * n), Wn(np * ptw), O(no * ctw);
-    for (std::size_t i = 0; i < na; i++) {
-        const Ciphertext &c = *cts[i];
-        if (c.parmsID() != first.parmsID() || c.size() != 2 || c.isNttForm() ||
-            c.correctionFactor() != first.correctionFactor())
-            throw std::invalid_argument("ciphertexts must be size-2, coefficient form, one level and correction factor");
-        cuda_ok(cudaMemcpyAsync(A.get() + i * ctw, c.data(), ctw * 8, cudaMemcpyDeviceToDevice, 0), "device copy");
+    for (const Ciphertext *c : cts)
+        if (c->parmsID() != first.parmsID() || c->size() != size || c->isNttForm() != ntt ||
+            c->correctionFactor() != first.correctionFactor())
+            throw std::invalid_argument("encrypted1 and encrypted2 parameter mismatch");
+    // An output's scale is its first product's (addInplace keeps the left operand's);
+    // NTT-form products multiply the scales, each within bounds as in multiplyPlain.
+    std::vector<double> scales(no);
+    for (std::size_t o = 0; o < no; o++) scales[o] = cts[ia[off[o]]]->scale();
+    if (ntt) {
+        for (const Plaintext *p : pts) {
+            if (!p->isNttForm() || p->parmsID() != first.parmsID())
+                throw std::invalid_argument("encrypted_ntt and plain_ntt parameter mismatch");
+            if (p->coeffCount() != ptw) throw std::invalid_argument("plain is not valid for encryption parameters");
+        }
+        for (std::size_t k = 0; k < ia.size(); k++)
+            if (!isScaleWithinBounds(cts[ia[k]]->scale() * pts[iw[k]]->scale(), *d))
+                throw std::invalid_argument("scale out of bounds");
+        for (std::size_t o = 0; o < no; o++) scales[o] *= pts[iw[off[o]]]->scale();
+    } else {
+        for (const Plaintext *p : pts)
+            if (p->isNttForm() || p->coeffCount() > n)
+                throw std::invalid_argument("plain is not valid for encryption parameters");
     }
-    Wr.zero();
-    for (std::size_t j = 0; j < np; j++) {
-        const Plaintext &pt = *pts[j];
-        if (pt.isNttForm() || pt.coeffCount() > n) throw std::invalid_argument("plaintexts must be in coefficient form");
-        if (pt.coeffCount())
-            cuda_ok(cudaMemcpyAsync(Wr.get() + j * n, pt.data(), pt.coeffCount() * 8, cudaMemcpyDeviceToDevice, 0),
+    DeviceBuffer A(na * ctw), Wn(np * ptw), O(no * ctw);
+    for (std::size_t i = 0; i < na; i++)
+        cuda_ok(cudaMemcpyAsync(A.get() + i * ctw, cts[i]->data(), ctw * 8, cudaMemcpyDeviceToDevice, 0),
+                "device copy");
+    tb_context *h = ctx.handle();
+    if (ntt) {
+        for (std::size_t j = 0; j < np; j++)
+            cuda_ok(cudaMemcpyAsync(Wn.get() + j * ptw, pts[j]->data(), ptw * 8, cudaMemcpyDeviceToDevice, 0),
                     "device copy");
+    } else {
+        DeviceBuffer Wr(np * n);
+        Wr.zero();
+        for (std::size_t j = 0; j < np; j++)
+            if (pts[j]->coeffCount())
+                cuda_ok(cudaMemcpyAsync(Wr.get() + j * n, pts[j]->data(), pts[j]->coeffCount() * 8,
+                                        cudaMemcpyDeviceToDevice, 0),
+                        "device copy");
+        tb_ok(tb_ntt_forward(h, A.get(), A.get(), size * na, 0, L, 0, nullptr));
+        tb_ok(tb_plain_to_ntt(h, L, Wr.get(), n, n, Wn.get(), np, nullptr));
     }
     DeviceBuffer doff = upload_u32(off), dia = upload_u32(ia), diw = upload_u32(iw);
-    tb_context *h = ctx.handle();
-    tb_ok(tb_ntt_forward(h, A.get(), A.get(), 2 * na, 0, L, 0, nullptr));
-    tb_ok(tb_plain_to_ntt(h, L, Wr.get(), n, n, Wn.get(), np, nullptr));
-    tb_ok(tb_dyadic_accumulate(h, L, 2, A.get(), 0, Wn.get(), 0, O.get(), 0, (const uint32_t *)doff.get(),
+    tb_ok(tb_dyadic_accumulate(h, L, (int)size, A.get(), 0, Wn.get(), 0, O.get(), 0, (const uint32_t *)doff.get(),
                                (const uint32_t *)dia.get(), (const uint32_t *)diw.get(), (uint32_t)no, nullptr));
-    tb_ok(tb_ntt_inverse(h, O.get(), O.get(), 2 * no, 0, L, 0, nullptr));
+    if (!ntt) tb_ok(tb_ntt_inverse(h, O.get(), O.get(), size * no, 0, L, 0, nullptr));
     std::vector<Ciphertext> out;
     out.reserve(no);
     for (std::size_t o = 0; o < no; o++) {
-        Ciphertext c(ctx, first.parmsID(), 2);
+        Ciphertext c(ctx, first.parmsID(), size);
         cuda_ok(cudaMemcpyAsync(c.data(), O.get() + o * ctw, ctw * 8, cudaMemcpyDeviceToDevice, 0), "device copy");
+        c.isNttForm() = ntt;
+        c.scale() = scales[o];
         c.correctionFactor() = first.correctionFactor();
         out.push_back(std::move(c));
     }
@@ -450,117 +469,102 @@ Plain2d MatmulHelper::deserializeEncodedWeights(std::istream &s) const {
     return out;
 }
 
-// ------------------------------------------------------------------ Conv2dHelper
+// ------------------------------------------------------------------ convolution geometry
 
-Conv2dHelper::Conv2dHelper(std::size_t batch, std::size_t image_height, std::size_t image_width,
-                           std::size_t kernel_height, std::size_t kernel_width, std::size_t input_channels,
-                           std::size_t output_channels, std::size_t slots)
-    : batch_(batch), kh_(kernel_height), kw_(kernel_width), ih_(image_height), iw_(image_width), ic_(input_channels),
-      oc_(output_channels), slots_(slots) {
-    if (!batch || !image_height || !image_width || !kernel_height || !kernel_width || !input_channels ||
-        !output_channels || !slots)
+ConvGeometry::ConvGeometry(std::size_t batch_, std::size_t ih_, std::size_t iw_, std::size_t kh_, std::size_t kw_,
+                           std::size_t ic_, std::size_t oc_, std::size_t slots_)
+    : batch(batch_), ih(ih_), iw(iw_), kh(kh_), kw(kw_), ic(ic_), oc(oc_), slots(slots_) {
+    if (!batch || !ih || !iw || !kh || !kw || !ic || !oc || !slots)
         throw std::invalid_argument("convolution dimensions must be positive");
-    if (kernel_height > image_height || kernel_width > image_width) throw std::invalid_argument("kernel larger than image");
+    if (kh > ih || kw > iw) throw std::invalid_argument("kernel larger than image");
     const std::size_t max_size = (std::size_t)std::sqrt((double)slots);
-    if (image_height > max_size || image_width > max_size) {
-        bh_ = bw_ = max_size;
-        blocked_ = true;
-    } else {
-        bh_ = image_height;
-        bw_ = image_width;
-        blocked_ = false;
-    }
-    if (blocked_ && (kernel_height > bh_ || kernel_width > bw_)) throw std::invalid_argument("kernel larger than a block");
+    blocked = ih > max_size || iw > max_size;
+    bh = blocked ? max_size : ih;
+    bw = blocked ? max_size : iw;
+    if (kh > bh || kw > bw) throw std::invalid_argument("kernel larger than a block");
 }
 
-std::size_t Conv2dHelper::totalBatchSize() const {
-    if (!blocked_) return batch_;
-    const std::size_t kh = kh_ - 1, kw = kw_ - 1;
-    return batch_ * ceil_div(ih_ - kh, bh_ - kh) * ceil_div(iw_ - kw, bw_ - kw);
-}
-
-// encodeWeights (app/LinearHelper.cuh:626-661): each output channel's kernels for a
-// group of input channels, reversed, in one coefficient-encoded plaintext.
-Plain2d Conv2dHelper::encodeWeights(const BatchEncoder &encoder, const std::vector<uint64_t> &weights) const {
-    if (weights.size() != ic_ * oc_ * kh_ * kw_) throw std::invalid_argument("Weights shape incorrect.");
-    const std::size_t block = bh_ * bw_, channel_slots = slots_ / block;
-    Plain2d out;
-    for (std::size_t oc = 0; oc < oc_; oc++) {
-        std::vector<Plaintext> row;
-        for (std::size_t lic = 0; lic < ic_; lic += channel_slots) {
-            const std::size_t uic = std::min(lic + channel_slots, ic_);
-            std::vector<uint64_t> spread(channel_slots * block, 0);
-            for (std::size_t j = lic; j < uic; j++)
-                for (std::size_t ki = 0; ki < kh_; ki++)
-                    for (std::size_t kj = 0; kj < kw_; kj++)
-                        spread[(channel_slots - 1 - (j - lic)) * block + ki * bw_ + kj] =
-                            weights[((oc * ic_) + j) * (kh_ * kw_) + (kh_ - ki - 1) * kw_ + (kw_ - kj - 1)];
-            Plaintext pt;
-            encoder.encodePolynomial(spread, pt);
-            row.push_back(std::move(pt));
+// encodeWeights (app/LinearHelper.cuh:626-661): channel j's kernel, flipped, at
+// channel slot channel_slots - 1 - (j - first channel of the group).
+template <class T>
+std::vector<std::vector<std::vector<T>>> ConvGeometry::weightVectors(const std::vector<T> &weights) const {
+    if (weights.size() != ic * oc * kh * kw) throw std::invalid_argument("Weights shape incorrect.");
+    const std::size_t blk = block(), cs = channelSlots();
+    std::vector<std::vector<std::vector<T>>> out(oc);
+    for (std::size_t o = 0; o < oc; o++)
+        for (std::size_t lic = 0; lic < ic; lic += cs) {
+            std::vector<T> spread(cs * blk, T(0));
+            for (std::size_t j = lic; j < std::min(lic + cs, ic); j++)
+                for (std::size_t ki = 0; ki < kh; ki++)
+                    for (std::size_t kj = 0; kj < kw; kj++)
+                        spread[(cs - 1 - (j - lic)) * blk + ki * bw + kj] =
+                            weights[((o * ic) + j) * (kh * kw) + (kh - ki - 1) * kw + (kw - kj - 1)];
+            out[o].push_back(std::move(spread));
         }
-        out.data.push_back(std::move(row));
-    }
     return out;
 }
 
-// encodeInputs (app/LinearHelper.cuh:674-740): blocks of the images (overlapping by
-// kernel - 1 when blocked), channel groups per plaintext.
-Plain2d Conv2dHelper::encodeInputs(const BatchEncoder &encoder, const std::vector<uint64_t> &inputs) const {
-    if (inputs.size() != batch_ * ic_ * ih_ * iw_) throw std::invalid_argument("Inputs shape incorrect.");
-    const std::size_t total = totalBatchSize(), block = bh_ * bw_;
-    std::vector<uint64_t> split;
-    if (!blocked_) {
-        split = inputs;
-    } else {
-        const std::size_t kh = kh_ - 1, kw = kw_ - 1;
-        const std::size_t sh = ceil_div(ih_ - kh, bh_ - kh), sw = ceil_div(iw_ - kw, bw_ - kw);
-        split.assign(batch_ * sh * sw * ic_ * block, 0);
-        const std::size_t image = ih_ * iw_;
-        for (std::size_t b = 0; b < batch_; b++)
-            for (std::size_t i = 0; i < sh; i++)
-                for (std::size_t j = 0; j < sw; j++) {
-                    const std::size_t bid = b * sh * sw + i * sw + j;
-                    const std::size_t si = i * (bh_ - kh), sj = j * (bw_ - kw);
-                    const std::size_t ui = (si + bh_ >= ih_) ? ih_ : (si + bh_);
-                    const std::size_t uj = (sj + bw_ >= iw_) ? iw_ : (sj + bw_);
-                    for (std::size_t tc = 0; tc < ic_; tc++)
+// encodeInputs (app/LinearHelper.cuh:674-742): block (b, i, j) starts at row
+// i * (bh - kh + 1), column j * (bw - kw + 1) of image b; channel c + k of a group at
+// channel slot k.
+template <class T>
+std::vector<std::vector<std::vector<T>>> ConvGeometry::inputVectors(const std::vector<T> &inputs) const {
+    if (inputs.size() != batch * ic * ih * iw) throw std::invalid_argument("Inputs shape incorrect.");
+    const std::size_t blk = block(), cs = channelSlots(), sh = splitsH(), sw = splitsW(), image = ih * iw;
+    std::vector<std::vector<std::vector<T>>> out;
+    out.reserve(totalBatchSize());
+    for (std::size_t b = 0; b < batch; b++)
+        for (std::size_t i = 0; i < sh; i++)
+            for (std::size_t j = 0; j < sw; j++) {
+                const std::size_t si = i * (bh - kh + 1), sj = j * (bw - kw + 1);
+                const std::size_t ui = std::min(si + bh, ih), uj = std::min(sj + bw, iw);
+                std::vector<std::vector<T>> groups;
+                for (std::size_t c = 0; c < ic; c += cs) {
+                    std::vector<T> plain(slots, T(0));
+                    for (std::size_t k = 0; k < std::min(cs, ic - c); k++)
                         for (std::size_t ti = 0; ti < ui - si; ti++)
                             for (std::size_t tj = 0; tj < uj - sj; tj++)
-                                split[bid * block * ic_ + tc * block + ti * bw_ + tj] =
-                                    inputs[b * image * ic_ + tc * image + (si + ti) * iw_ + (sj + tj)];
+                                plain[k * blk + ti * bw + tj] =
+                                    inputs[b * image * ic + (c + k) * image + (si + ti) * iw + (sj + tj)];
+                    groups.push_back(std::move(plain));
                 }
-    }
-    const std::size_t channel_slots = slots_ / block;
-    Plain2d out;
-    for (std::size_t b = 0; b < total; b++) {
-        std::vector<Plaintext> group;
-        for (std::size_t c = 0; c < ic_; c += channel_slots) {
-            const std::size_t upper = std::min(c + channel_slots, ic_);
-            std::vector<uint64_t> plain(slots_, 0);
-            for (std::size_t k = 0; k < upper - c; k++)
-                for (std::size_t i = 0; i < bh_; i++)
-                    for (std::size_t j = 0; j < bw_; j++)
-                        plain[k * block + i * bw_ + j] = split[b * ic_ * block + (c + k) * block + i * bw_ + j];
-            Plaintext pt;
-            encoder.encodePolynomial(plain, pt);
-            group.push_back(std::move(pt));
-        }
-        out.data.push_back(std::move(group));
-    }
+                out.push_back(std::move(groups));
+            }
     return out;
 }
 
-Cipher2d Conv2dHelper::encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder,
-                                     const std::vector<uint64_t> &inputs) const {
-    return encodeInputs(encoder, inputs).encrypt(encryptor);
+// decryptOutputs (app/LinearHelper.cuh:886-930): output (i, j) of block b sits at
+// (channel_slots - 1) * block + (bh - yh + i) * bw + (bw - yw + j).
+std::vector<std::pair<std::size_t, std::size_t>> ConvGeometry::outputMap(std::size_t b, std::size_t c) const {
+    const std::size_t yh = bh - kh + 1, yw = bw - kw + 1, oyh = ih - kh + 1, oyw = iw - kw + 1;
+    const std::size_t sh = splitsH(), sw = splitsW();
+    const std::size_t ob = b / (sh * sw), si = (b % (sh * sw)) / sw, sj = b % sw;
+    std::vector<std::pair<std::size_t, std::size_t>> m;
+    for (std::size_t i = 0; i < yh; i++)
+        for (std::size_t j = 0; j < yw; j++)
+            if (si * yh + i < oyh && sj * yw + j < oyw)
+                m.emplace_back((channelSlots() - 1) * block() + (bh - yh + i) * bw + (bw - yw + j),
+                               ob * oc * oyh * oyw + c * oyh * oyw + (si * yh + i) * oyw + (sj * yw + j));
+    return m;
 }
 
+std::vector<std::size_t> ConvGeometry::outputTerms() const {
+    const std::size_t st = (channelSlots() - 1) * block();
+    std::vector<std::size_t> r(block());
+    for (std::size_t i = 0; i < r.size(); i++) r[i] = st + i;
+    return r;
+}
+
+template std::vector<std::vector<std::vector<uint64_t>>> ConvGeometry::weightVectors(const std::vector<uint64_t> &) const;
+template std::vector<std::vector<std::vector<double>>> ConvGeometry::weightVectors(const std::vector<double> &) const;
+template std::vector<std::vector<std::vector<uint64_t>>> ConvGeometry::inputVectors(const std::vector<uint64_t> &) const;
+template std::vector<std::vector<std::vector<double>>> ConvGeometry::inputVectors(const std::vector<double> &) const;
+
 // conv2d (app/LinearHelper.cuh:752-773): output (b, oc) = sum_i a[b][i] * w[oc][i].
-Cipher2d Conv2dHelper::conv2d(const Evaluator &ev, const Cipher2d &a, const Plain2d &w) const {
-    const std::size_t total = totalBatchSize();
+Cipher2d convolve(const Evaluator &ev, const ConvGeometry &g, const Cipher2d &a, const Plain2d &w) {
+    const std::size_t total = g.totalBatchSize();
     if (a.data.size() != total) throw std::invalid_argument("Input batchsize incorrect.");
-    if (w.data.size() != oc_) throw std::invalid_argument("Weight output channels incorrect.");
+    if (w.data.size() != g.oc) throw std::invalid_argument("Weight output channels incorrect.");
     const std::size_t groups = a[0].size();
     std::vector<const Ciphertext *> cts;
     std::vector<const Plaintext *> pts;
@@ -574,7 +578,7 @@ Cipher2d Conv2dHelper::conv2d(const Evaluator &ev, const Cipher2d &a, const Plai
     }
     std::vector<uint32_t> off{0}, ia, iw;
     for (std::size_t b = 0; b < total; b++)
-        for (std::size_t oc = 0; oc < oc_; oc++) {
+        for (std::size_t oc = 0; oc < g.oc; oc++) {
             for (std::size_t i = 0; i < groups; i++) {
                 ia.push_back((uint32_t)(b * groups + i));
                 iw.push_back((uint32_t)(oc * groups + i));
@@ -585,19 +589,56 @@ Cipher2d Conv2dHelper::conv2d(const Evaluator &ev, const Cipher2d &a, const Plai
     Cipher2d out;
     out.data.resize(total);
     for (std::size_t b = 0; b < total; b++)
-        for (std::size_t oc = 0; oc < oc_; oc++) out.data[b].push_back(std::move(flat[b * oc_ + oc]));
+        for (std::size_t oc = 0; oc < g.oc; oc++) out.data[b].push_back(std::move(flat[b * g.oc + oc]));
     return out;
+}
+
+// ------------------------------------------------------------------ Conv2dHelper
+
+namespace {
+
+Plain2d encode_rows(const BatchEncoder &encoder, const std::vector<std::vector<std::vector<uint64_t>>> &rows) {
+    Plain2d out;
+    for (auto &r : rows) {
+        std::vector<Plaintext> row;
+        for (auto &v : r) {
+            Plaintext pt;
+            encoder.encodePolynomial(v, pt);
+            row.push_back(std::move(pt));
+        }
+        out.data.push_back(std::move(row));
+    }
+    return out;
+}
+
+}  // namespace
+
+Plain2d Conv2dHelper::encodeWeights(const BatchEncoder &encoder, const std::vector<uint64_t> &weights) const {
+    return encode_rows(encoder, g_.weightVectors(weights));
+}
+
+Plain2d Conv2dHelper::encodeInputs(const BatchEncoder &encoder, const std::vector<uint64_t> &inputs) const {
+    return encode_rows(encoder, g_.inputVectors(inputs));
+}
+
+Cipher2d Conv2dHelper::encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder,
+                                     const std::vector<uint64_t> &inputs) const {
+    return encodeInputs(encoder, inputs).encrypt(encryptor);
+}
+
+Cipher2d Conv2dHelper::conv2d(const Evaluator &ev, const Cipher2d &a, const Plain2d &w) const {
+    return convolve(ev, g_, a, w);
 }
 
 // conv2dCipher (app/LinearHelper.cuh:775-797): ciphertext kernels, one multiply and
 // addInplace per pair as the reference.
 Cipher2d Conv2dHelper::conv2dCipher(const Evaluator &ev, const Cipher2d &a, const Cipher2d &w) const {
-    const std::size_t total = totalBatchSize();
+    const std::size_t total = g_.totalBatchSize();
     if (a.data.size() != total) throw std::invalid_argument("Input batchsize incorrect.");
     Cipher2d out;
     for (std::size_t b = 0; b < total; b++) {
         std::vector<Ciphertext> group;
-        for (std::size_t oc = 0; oc < oc_; oc++) {
+        for (std::size_t oc = 0; oc < g_.oc; oc++) {
             Ciphertext acc;
             for (std::size_t i = 0; i < a[b].size(); i++) {
                 Ciphertext prod;
@@ -616,9 +657,9 @@ Cipher2d Conv2dHelper::conv2dCipher(const Evaluator &ev, const Cipher2d &a, cons
 
 // conv2dReverse (app/LinearHelper.cuh:799-820): plaintext images, ciphertext kernels.
 Cipher2d Conv2dHelper::conv2dReverse(const Evaluator &ev, const Plain2d &a, const Cipher2d &w) const {
-    const std::size_t total = totalBatchSize();
+    const std::size_t total = g_.totalBatchSize();
     if (a.data.size() != total) throw std::invalid_argument("Input batchsize incorrect.");
-    if (w.data.size() != oc_) throw std::invalid_argument("Weight output channels incorrect.");
+    if (w.data.size() != g_.oc) throw std::invalid_argument("Weight output channels incorrect.");
     const std::size_t groups = a[0].size();
     std::vector<const Ciphertext *> cts;
     std::vector<const Plaintext *> pts;
@@ -632,7 +673,7 @@ Cipher2d Conv2dHelper::conv2dReverse(const Evaluator &ev, const Plain2d &a, cons
     }
     std::vector<uint32_t> off{0}, ia, iw;
     for (std::size_t b = 0; b < total; b++)
-        for (std::size_t oc = 0; oc < oc_; oc++) {
+        for (std::size_t oc = 0; oc < g_.oc; oc++) {
             for (std::size_t i = 0; i < groups; i++) {
                 ia.push_back((uint32_t)(oc * groups + i));
                 iw.push_back((uint32_t)(b * groups + i));
@@ -643,30 +684,20 @@ Cipher2d Conv2dHelper::conv2dReverse(const Evaluator &ev, const Plain2d &a, cons
     Cipher2d out;
     out.data.resize(total);
     for (std::size_t b = 0; b < total; b++)
-        for (std::size_t oc = 0; oc < oc_; oc++) out.data[b].push_back(std::move(flat[b * oc_ + oc]));
+        for (std::size_t oc = 0; oc < g_.oc; oc++) out.data[b].push_back(std::move(flat[b * g_.oc + oc]));
     return out;
 }
 
-// encodeOutputs / decryptOutputs (app/LinearHelper.cuh:822-930): the valid output
-// window sits in the last channel slot of each output polynomial.
+// encodeOutputs (app/LinearHelper.cuh:822-861). As the reference, one mask vector is
+// reused across outputs, so positions a later block does not hold keep earlier values.
 Plain2d Conv2dHelper::encodeOutputs(const BatchEncoder &encoder, const std::vector<uint64_t> &outputs) const {
-    const std::size_t block = bh_ * bw_, channel_slots = slots_ / block;
-    const std::size_t yh = bh_ - kh_ + 1, yw = bw_ - kw_ + 1, oyh = ih_ - kh_ + 1, oyw = iw_ - kw_ + 1;
-    if (outputs.size() != batch_ * oc_ * oyh * oyw) throw std::invalid_argument("Outputs shape incorrect.");
-    const std::size_t kh = kh_ - 1, kw = kw_ - 1;
-    const std::size_t sh = ceil_div(ih_ - kh, bh_ - kh), sw = ceil_div(iw_ - kw, bw_ - kw);
-    std::vector<uint64_t> mask(channel_slots * block, 0);
+    if (outputs.size() != g_.outputCount()) throw std::invalid_argument("Outputs shape incorrect.");
+    std::vector<uint64_t> mask(g_.channelSlots() * g_.block(), 0);
     Plain2d out;
-    for (std::size_t b = 0; b < totalBatchSize(); b++) {
-        const std::size_t ob = b / (sh * sw), si = (b % (sh * sw)) / sw, sj = b % sw;
+    for (std::size_t b = 0; b < g_.totalBatchSize(); b++) {
         std::vector<Plaintext> group;
-        for (std::size_t c = 0; c < oc_; c++) {
-            for (std::size_t i = 0; i < yh; i++)
-                for (std::size_t j = 0; j < yw; j++) {
-                    const std::size_t mi = (channel_slots - 1) * block + (bh_ - yh + i) * bw_ + (bw_ - yw + j);
-                    if (si * yh + i < oyh && sj * yw + j < oyw)
-                        mask[mi] = outputs[ob * oc_ * oyh * oyw + c * oyh * oyw + (si * yh + i) * oyw + (sj * yw + j)];
-                }
+        for (std::size_t c = 0; c < g_.oc; c++) {
+            for (auto &[mi, oi] : g_.outputMap(b, c)) mask[mi] = outputs[oi];
             Plaintext pt;
             encoder.encodePolynomial(mask, pt);
             group.push_back(std::move(pt));
@@ -678,46 +709,31 @@ Plain2d Conv2dHelper::encodeOutputs(const BatchEncoder &encoder, const std::vect
 
 std::vector<uint64_t> Conv2dHelper::decryptOutputs(const BatchEncoder &encoder, Decryptor &decryptor,
                                                    const Cipher2d &outputs) const {
-    const std::size_t block = bh_ * bw_, channel_slots = slots_ / block;
-    const std::size_t yh = bh_ - kh_ + 1, yw = bw_ - kw_ + 1, oyh = ih_ - kh_ + 1, oyw = iw_ - kw_ + 1;
-    const std::size_t kh = kh_ - 1, kw = kw_ - 1;
-    const std::size_t sh = ceil_div(ih_ - kh, bh_ - kh), sw = ceil_div(iw_ - kw, bw_ - kw);
-    std::vector<uint64_t> ret(batch_ * oc_ * oyh * oyw);
-    for (std::size_t b = 0; b < totalBatchSize(); b++) {
-        const std::size_t ob = b / (sh * sw), si = (b % (sh * sw)) / sw, sj = b % sw;
-        for (std::size_t c = 0; c < oc_; c++) {
+    std::vector<uint64_t> ret(g_.outputCount());
+    for (std::size_t b = 0; b < g_.totalBatchSize(); b++)
+        for (std::size_t c = 0; c < g_.oc; c++) {
             Plaintext pt;
             decryptor.decrypt(outputs.data.at(b).at(c), pt);
             std::vector<uint64_t> buf;
             encoder.decodePolynomial(pt, buf);
-            for (std::size_t i = 0; i < yh; i++)
-                for (std::size_t j = 0; j < yw; j++) {
-                    const std::size_t mi = (channel_slots - 1) * block + (bh_ - yh + i) * bw_ + (bw_ - yw + j);
-                    if (si * yh + i < oyh && sj * yw + j < oyw)
-                        ret[ob * oc_ * oyh * oyw + c * oyh * oyw + (si * yh + i) * oyw + (sj * yw + j)] = buf[mi];
-                }
+            for (auto &[mi, oi] : g_.outputMap(b, c)) ret[oi] = buf[mi];
         }
-    }
     return ret;
 }
 
 // serializeOutputs / deserializeOutputs (app/LinearHelper.cuh:932-972): the whole last
 // channel slot of every output travels.
 void Conv2dHelper::serializeOutputs(const Evaluator &ev, const Cipher2d &x, std::ostream &s) const {
-    const std::size_t block = bh_ * bw_, channel_slots = slots_ / block, st = (channel_slots - 1) * block;
-    std::vector<std::size_t> required(block);
-    for (std::size_t i = 0; i < block; i++) required[i] = st + i;
-    for (std::size_t b = 0; b < totalBatchSize(); b++)
-        for (std::size_t oc = 0; oc < oc_; oc++) x.data.at(b).at(oc).saveTerms(s, ev, required);
+    const auto required = g_.outputTerms();
+    for (std::size_t b = 0; b < g_.totalBatchSize(); b++)
+        for (std::size_t oc = 0; oc < g_.oc; oc++) x.data.at(b).at(oc).saveTerms(s, ev, required);
 }
 
 Cipher2d Conv2dHelper::deserializeOutputs(const Evaluator &ev, std::istream &s) const {
-    const std::size_t block = bh_ * bw_, channel_slots = slots_ / block, st = (channel_slots - 1) * block;
-    std::vector<std::size_t> required(block);
-    for (std::size_t i = 0; i < block; i++) required[i] = st + i;
+    const auto required = g_.outputTerms();
     Cipher2d out;
-    for (std::size_t b = 0; b < totalBatchSize(); b++) {
-        std::vector<Ciphertext> row(oc_);
+    for (std::size_t b = 0; b < g_.totalBatchSize(); b++) {
+        std::vector<Ciphertext> row(g_.oc);
         for (auto &c : row) c.loadTerms(s, ev, required);
         out.data.push_back(std::move(row));
     }

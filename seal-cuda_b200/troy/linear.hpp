@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <iosfwd>
+#include <utility>
 #include <vector>
 
 #include "troy_b200.hpp"
@@ -42,8 +43,13 @@ public:
 };
 
 // Sums of ciphertext x plaintext products on the device: output o is
-// sum_{k in [off[o], off[o+1])} cts[ia[k]] * pts[iw[k]] (BFV/BGV, coefficient-form
-// size-2 ciphertexts of one level and correction factor, coefficient plaintexts).
+// sum_{k in [off[o], off[o+1])} cts[ia[k]] * pts[iw[k]], the words of the reference's
+// multiplyPlain of each pair followed by addInplace. The ciphertexts share level, size,
+// form, scale and correction factor. Coefficient-form ciphertexts (BFV/BGV) take
+// coefficient plaintexts: each ciphertext and plaintext is transformed once, one
+// inverse transform per output. NTT-form ciphertexts (CKKS, or BFV/BGV after
+// transformToNtt) take NTT plaintexts of the same parms_id and scale, multiplied in
+// place with no transform at all.
 std::vector<Ciphertext> sumOfProducts(const Evaluator &evaluator, const std::vector<const Ciphertext *> &cts,
                                       const std::vector<const Plaintext *> &pts, const std::vector<uint32_t> &off,
                                       const std::vector<uint32_t> &ia, const std::vector<uint32_t> &iw);
@@ -86,6 +92,32 @@ private:
     MatmulPlan plan_;
 };
 
+// Geometry shared by the convolution helpers (app/LinearHelper.cuh:531-975 and
+// app/LinearHelperCKKS.cuh:362-716): images larger than sqrt(slots) split into blocks
+// that overlap by kernel - 1; `channel_slots` input channels share one polynomial.
+struct ConvGeometry {
+    std::size_t batch, ih, iw, kh, kw, ic, oc, slots, bh, bw;
+    bool blocked;
+    ConvGeometry(std::size_t batch, std::size_t ih, std::size_t iw, std::size_t kh, std::size_t kw, std::size_t ic,
+                 std::size_t oc, std::size_t slots);
+    std::size_t block() const { return bh * bw; }
+    std::size_t channelSlots() const { return slots / block(); }
+    std::size_t splitsH() const { return (ih - kh + 1 + bh - kh) / (bh - kh + 1); }
+    std::size_t splitsW() const { return (iw - kw + 1 + bw - kw) / (bw - kw + 1); }
+    std::size_t totalBatchSize() const { return blocked ? batch * splitsH() * splitsW() : batch; }
+    std::size_t outputCount() const { return batch * oc * (ih - kh + 1) * (iw - kw + 1); }
+    // coefficient vectors: [output channel][channel group] of flipped kernels, and
+    // [block][channel group] of image blocks
+    template <class T>
+    std::vector<std::vector<std::vector<T>>> weightVectors(const std::vector<T> &weights) const;
+    template <class T>
+    std::vector<std::vector<std::vector<T>>> inputVectors(const std::vector<T> &inputs) const;
+    // (coefficient, output index) of every output held by block b's polynomials
+    std::vector<std::pair<std::size_t, std::size_t>> outputMap(std::size_t b, std::size_t channel) const;
+    // the last channel slot, which every output polynomial's outputs lie in
+    std::vector<std::size_t> outputTerms() const;
+};
+
 // Conv2dHelper (app/LinearHelper.cuh:531-975): a "valid" 2-d convolution of
 // batch x input-channels x height x width images with output-channels x
 // input-channels x kh x kw kernels; images larger than sqrt(slots) are split into
@@ -94,8 +126,9 @@ class Conv2dHelper {
 public:
     Conv2dHelper(std::size_t batch, std::size_t image_height, std::size_t image_width, std::size_t kernel_height,
                  std::size_t kernel_width, std::size_t input_channels, std::size_t output_channels,
-                 std::size_t slots);
-    std::size_t totalBatchSize() const;
+                 std::size_t slots)
+        : g_(batch, image_height, image_width, kernel_height, kernel_width, input_channels, output_channels, slots) {}
+    std::size_t totalBatchSize() const { return g_.totalBatchSize(); }
     Plain2d encodeWeights(const BatchEncoder &encoder, const std::vector<std::uint64_t> &weights) const;
     Plain2d encodeInputs(const BatchEncoder &encoder, const std::vector<std::uint64_t> &inputs) const;
     Cipher2d encryptInputs(const Encryptor &encryptor, const BatchEncoder &encoder,
@@ -112,8 +145,19 @@ public:
     Cipher2d deserializeOutputs(const Evaluator &evaluator, std::istream &stream) const;
 
 private:
-    std::size_t batch_, bh_, bw_, kh_, kw_, ih_, iw_, ic_, oc_, slots_;
-    bool blocked_;
+    ConvGeometry g_;
 };
 
+// Output (b, o) = sum over channel groups i of a[b][i] * w[o][i] (the convolution
+// helpers' sums), fused.
+Cipher2d convolve(const Evaluator &evaluator, const ConvGeometry &g, const Cipher2d &a, const Plain2d &w);
+
 }  // namespace troyn
+
+// The reference's namespace for these classes (app/LinearHelper.cuh:7).
+namespace LinearHelper {
+using troyn::Cipher2d;
+using troyn::Conv2dHelper;
+using troyn::MatmulHelper;
+using troyn::Plain2d;
+}  // namespace LinearHelper

@@ -1,6 +1,8 @@
 // The continuous-batching MatmulServer over the library's batched device operations.
 #include "serving.hpp"
 
+#include "device_util.hpp"
+
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
@@ -12,9 +14,7 @@ namespace troyn {
 
 namespace {
 
-void cuda_ok(cudaError_t e, const char *what) {
-    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
+using detail::cuda_ok;
 
 // Record of tb_matmul_encode_weights: {offset lo, offset hi, in, out, ib, ob, li, lj}.
 void push_block(std::vector<uint32_t> &d, uint64_t src, const MatmulPlan &p, std::size_t bi, std::size_t bj) {

@@ -543,11 +543,9 @@ void Decryptor::decrypt(const Ciphertext &ct, Plaintext &dest) {
 
 // ------------------------------------------------------------------ evaluator helpers
 
-namespace {
-
 // isScaleWithinBounds (src/evaluator_cuda.cu): log2(scale) below the plain modulus
 // bits (BFV/BGV) or the level's total modulus bits (CKKS).
-bool scale_ok(double scale, const SEALContext::ContextData &d) {
+bool isScaleWithinBounds(double scale, const SEALContext::ContextData &d) {
     int bound = 0;
     switch (d.parms().scheme()) {
     case SchemeType::bfv:
@@ -562,6 +560,10 @@ bool scale_ok(double scale, const SEALContext::ContextData &d) {
     }
     return !(scale <= 0 || (int)std::log2(scale) >= bound);
 }
+
+namespace {
+
+bool scale_ok(double scale, const SEALContext::ContextData &d) { return isScaleWithinBounds(scale, d); }
 
 // Relative closeness of two scales (areClose, src/utils/common.h).
 bool same_scale(double a, double b) {

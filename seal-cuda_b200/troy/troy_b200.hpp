@@ -331,6 +331,10 @@ public:
     bool hasKeyElt(std::uint32_t galois_elt) const { return hasKey(getIndex(galois_elt)); }
 };
 
+// isScaleWithinBounds (src/evaluator_cuda.cu): log2(scale) below the plain modulus
+// bits (BFV/BGV) or the level's total modulus bits (CKKS).
+bool isScaleWithinBounds(double scale, const SEALContext::ContextData &context_data);
+
 class KeyGenerator {
 public:
     explicit KeyGenerator(const SEALContext &context);

@@ -10,7 +10,7 @@ with the restatement."""
 import numpy as np
 import pytest
 
-from linear_layout import Conv2dLayout, MatmulLayout, negacyclic_mul
+from linear_layout import Conv2dLayout, DiagonalLayout, MatmulLayout, negacyclic_mul
 
 T = 65537
 
@@ -71,3 +71,27 @@ def test_conv2d_helper_host_parts():
     with pytest.raises(ValueError):
         pytroy.Conv2dHelper(0, 8, 8, 3, 3, 1, 1, 8192)
     assert len(pytroy.Cipher2d()) == 0 and len(pytroy.Plain2d()) == 0
+
+
+@pytest.mark.parametrize("height,width,slots", [(20, 30, 256), (500, 30, 4096), (60, 7, 64), (64, 64, 64)])
+def test_diagonal_layout_computes_the_matrix_vector_product(height, width, slots):
+    lay = DiagonalLayout(height, width, slots)
+    rng = np.random.default_rng(height * width)
+    m = rng.uniform(-1, 1, (height, width)) + 1j * rng.uniform(-1, 1, (height, width))
+    v = rng.uniform(-1, 1, width) + 1j * rng.uniform(-1, 1, width)
+    assert np.allclose(lay.apply(m, v), m @ v, atol=1e-12)
+    pytroy = pytest.importorskip("pytroy")
+    h = pytroy.DiagonalMatmulHelper(height, width, slots)
+    assert (h.pack_num, h.cipher_count) == (lay.pack, lay.count)
+
+
+def test_diagonal_helper_rejects_shapes_the_packing_cannot_hold():
+    """More diagonals than next_pow2(width) slots (here 16 > 8) lose rows in the packing
+    (the repacked diagonal index never reaches them), so such shapes are refused."""
+    pytroy = pytest.importorskip("pytroy")
+    lay = DiagonalLayout(100, 7, 64)
+    assert lay.count > lay.p2
+    with pytest.raises(ValueError):
+        pytroy.DiagonalMatmulHelper(100, 7, 64)
+    with pytest.raises(ValueError):
+        pytroy.DiagonalMatmulHelper(4, 100, 64)   # width beyond the slots
