@@ -313,6 +313,15 @@ def run_ntt_sweep(batch=256, reps=10):
             torch.cuda.synchronize()
             return e0.elapsed_time(e1) / reps
 
+        # the autotuner picks the launch variant per direction for this degree (restored
+        # afterwards, so the sweep leaves the other workloads' choices alone)
+        saved = []
+        for fwd in (1, 0):
+            v = ctypes.c_int(0)
+            lib.tb_ntt_get_variant(fwd, min(logn, 14), ctypes.byref(v))
+            saved.append(v.value)
+        vf, vi = ctypes.c_int(0), ctypes.c_int(0)
+        ctx("autotune_ntt", batch * 8, stream, ctypes.byref(vf), ctypes.byref(vi))
         words = batch * 8 * n
         ms_f = timed(lambda: ctx("ntt_forward", x, x, batch, 0, 8, 0, stream))
         ms_d = timed(lambda: ctx("dyadic_product", x, y, z, batch, 0, 8, stream))
@@ -322,7 +331,10 @@ def run_ntt_sweep(batch=256, reps=10):
                                  ("ntt_inverse", ms_i, 16 * words)):
             gbs = bytes_ / (ms * 1e-3) / 1e9
             row[name] = {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4)}
+        row["variants"] = {"forward": vf.value, "inverse": vi.value}
         out[f"N={n}"] = row
+        for fwd, v in zip((1, 0), saved):
+            lib.tb_ntt_set_variant(fwd, min(logn, 14), v)
         del x, y, z
         ctx.close()
     return {"workload": f"{batch} polynomials x 8 limbs (50-bit primes)", "results": out}

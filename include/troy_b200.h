@@ -352,12 +352,14 @@ int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_st
  * (its kernels have fixed launch shapes). Settings are process-wide.
  */
 
-/* NTT launch variant for one direction and log2 block size (12..14 have variants 0
-   and 1: the default thread count, and half of it with two radix-8 groups per thread). */
+/* NTT launch variant for one direction and log2 block size (12..14 have variants 0, 1
+   and 2: the default thread count, half and a quarter of it, each thread taking
+   correspondingly more radix-8 groups per pass; fewer threads let several limbs share
+   an SM). */
 int tb_ntt_set_variant(int forward, int log_block, int variant);
 int tb_ntt_get_variant(int forward, int log_block, int *variant);
-/* Times both variants of the context's transform size on `polys` scratch limbs (0 =
-   256) with CUDA events on `stream` and keeps the faster per direction. */
+/* Times every variant of the context's transform size on `polys` scratch limbs (0 =
+   256) with CUDA events on `stream` and keeps the fastest per direction. */
 int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_variant, int *inverse_variant);
 /* Scratch budget of one key-switch launch sequence: a batch whose intermediates exceed
    it is processed in chunks (default 2 GiB, or the TB_KS_SCRATCH_BYTES environment

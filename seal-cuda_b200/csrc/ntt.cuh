@@ -35,8 +35,12 @@ struct NttLimb {
 
 // Threads per CTA: variant 0 gives each thread one radix-8 group per pass at a time (at
 // most 1024 threads); variant V >= 1 divides the thread count by 2^V, each thread then
-// running its groups of a pass side by side (more independent work per thread, more
-// registers per thread). The variant per block size is a tuning choice (tb_ntt_*).
+// running more groups of a pass one after another. Fewer threads need fewer registers
+// per CTA, so several CTAs (limbs) share an SM and one CTA's barriers and memory
+// phases overlap another's arithmetic. The variant per block size is a tuning choice
+// (tb_ntt_*).
+constexpr int NTT_VARIANTS = 3;
+
 template <int LOGB, int V = 0>
 struct NttCfg {
     static constexpr int NB = 1 << LOGB;
@@ -44,6 +48,10 @@ struct NttCfg {
     static constexpr int THREADS = (BASE >> V) >= 32 ? (BASE >> V) : 32;
     static constexpr int REM = LOGB % 3;
 };
+
+// Shared-memory slot of coefficient base | (k << logsub) when the bits of k << logsub
+// are clear in base: swz(base) ^ swz_delta(k << logsub), a compile-time constant per k.
+__host__ __device__ constexpr int swz_delta(int kk) { return kk ^ ((kk >> 4) & 15); }
 
 __device__ __forceinline__ void ct_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     uint64_t u = x >= q2 ? x - q2 : x;
@@ -83,11 +91,11 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
             const int g = threadIdx.x + (i0 + it) * T;
             if (!FULL && g >= G) continue;
             const int base = ((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1));
+            const int sb = swz(base);
 #pragma unroll
             for (int k = 0; k < R; k++) {
-                const int e = base + (k << logsub);
-                if constexpr (FROM_GLOBAL) v[it][k] = op.load(c, e);
-                else v[it][k] = sm[swz(e)];
+                if constexpr (FROM_GLOBAL) v[it][k] = op.load(c, base + (k << logsub));
+                else v[it][k] = sm[sb ^ swz_delta(k << logsub)];
             }
         }
 #pragma unroll
@@ -98,11 +106,11 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 #pragma unroll
             for (int t = 0; t < R_LOG; t++) {
                 const int half = R >> (t + 1);
+                const ulonglong2 *row = c.lm.roots + (X << t);   // this stage's twiddles
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     if (k & half) continue;
-                    const uint32_t ri = (X << t) + (uint32_t)(k >> (R_LOG - t));
-                    ct_butterfly(v[it][k], v[it][k + half], __ldg(&c.lm.roots[ri]), q, q2);
+                    ct_butterfly(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
                 }
             }
         }
@@ -110,9 +118,9 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
         for (int it = 0; it < GR; it++) {
             const int g = threadIdx.x + (i0 + it) * T;
             if (!FULL && g >= G) continue;
-            const int base = ((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1));
+            const int sb = swz(((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1)));
 #pragma unroll
-            for (int k = 0; k < R; k++) sm[swz(base + (k << logsub))] = v[it][k];
+            for (int k = 0; k < R; k++) sm[sb ^ swz_delta(k << logsub)] = v[it][k];
         }
     }
     __syncthreads();
@@ -137,8 +145,8 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op
     const auto c = op.ctx(blockIdx.x);
     const uint32_t rbase = (1u << s0) + c.lm.sb;
     constexpr int FIRST = REM != 0 ? REM : 3;
-    fwd_pass<FIRST, true, LOGB, T, 0, (V > 0)>(op, c, sm, rbase);
-    fwd_passes<FIRST, LOGB, T, (V > 0)>(op, c, sm, rbase);
+    fwd_pass<FIRST, true, LOGB, T, 0, false>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
     // coalesced copy-out, two coefficients per thread
     for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
         const int p = swz(e);
@@ -169,9 +177,9 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
         for (int it = 0; it < GR; it++) {
             const int g = threadIdx.x + (i0 + it) * T;
             if (!FULL && g >= G) continue;
-            const int base = ((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1));
+            const int sb = swz(((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1)));
 #pragma unroll
-            for (int k = 0; k < R; k++) v[it][k] = sm[swz(base + (k << s))];
+            for (int k = 0; k < R; k++) v[it][k] = sm[sb ^ swz_delta(k << s)];
         }
 #pragma unroll
         for (int it = 0; it < GR; it++) {
@@ -195,8 +203,7 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
                         v[it][k] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
                         v[it][k + h] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
                     } else {
-                        const uint32_t ri = rb + (uint32_t)(k >> (t + 1));
-                        gs_butterfly(v[it][k], v[it][k + h], __ldg(&c.lm.iroots[ri]), q, q2);
+                        gs_butterfly(v[it][k], v[it][k + h], __ldg(c.lm.iroots + rb + (k >> (t + 1))), q, q2);
                     }
                 }
             }
@@ -206,11 +213,11 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
             const int g = threadIdx.x + (i0 + it) * T;
             if (!FULL && g >= G) continue;
             const int base = ((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1));
+            const int sb = swz(base);
 #pragma unroll
             for (int k = 0; k < R; k++) {
-                const int e = base + (k << s);
-                if constexpr (TO_GLOBAL) op.store(c, e, v[it][k]);
-                else sm[swz(e)] = v[it][k];
+                if constexpr (TO_GLOBAL) op.store(c, base + (k << s), v[it][k]);
+                else sm[sb ^ swz_delta(k << s)] = v[it][k];
             }
         }
     }
@@ -246,9 +253,9 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op
     __syncthreads();
     constexpr int LAST = REM ? REM : 3;
     constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;  // radix-8 passes before the last one
-    inv_passes<0, PASSES, LOGB, T, (V > 0)>(op, c, sm, logn);
-    if (scale_last) inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, (V > 0)>(op, c, sm, logn);
-    else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, (V > 0)>(op, c, sm, logn);
+    inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, logn);
+    if (scale_last) inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
+    else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
 }
 
 template <int LOGB>
@@ -305,17 +312,23 @@ inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int
     else return launch_inv<LOGB, V>(op, blocks, s0_or_logn, scale_last, s);
 }
 
-// Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry a second
-// variant with half the threads.
+// Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry variants
+// with half and a quarter of the threads.
 template <bool FWD, class Op>
 cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
 #define TB_CASE(B) \
     case B:        \
         return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);
-#define TB_CASE2(B)                                                                                  \
-    case B:                                                                                          \
-        if (ntt_variant(FWD, B) == 1) return launch_ntt<FWD, B, 1>(op, blocks, s0_or_logn, scale_last, s); \
-        return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);
+#define TB_CASE2(B)                                                                  \
+    case B:                                                                          \
+        switch (ntt_variant(FWD, B)) {                                               \
+        case 1:                                                                      \
+            return launch_ntt<FWD, B, 1>(op, blocks, s0_or_logn, scale_last, s);     \
+        case 2:                                                                      \
+            return launch_ntt<FWD, B, 2>(op, blocks, s0_or_logn, scale_last, s);     \
+        default:                                                                     \
+            return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);     \
+        }
     switch (logb) {
         TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
         TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE2(12) TB_CASE2(13) TB_CASE2(14)

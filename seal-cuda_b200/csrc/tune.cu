@@ -62,8 +62,8 @@ static float time_call(F &&f, cudaStream_t s, int reps, int &status) {
     return ms[ms.size() / 2];
 }
 
-// Times both variants of the forward and inverse transform of the context's degree
-// on `polys` limbs of scratch and keeps the faster of each.
+// Times every variant of the forward and inverse transform of the context's degree
+// on `polys` limbs of scratch and keeps the fastest of each.
 int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, int *chosen_inv) {
     const int logb = c.logn;
     if (logb < 12 || logb > MAX_LOGB) {
@@ -82,7 +82,7 @@ int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, in
     for (int dir = 1; dir >= 0 && st == TB_OK; dir--) {
         float best = 0;
         int best_v = 0;
-        for (int v = 0; v <= 1 && st == TB_OK; v++) {
+        for (int v = 0; v < NTT_VARIANTS && st == TB_OK; v++) {
             g_variant[dir][logb].store(v);
             const float t = time_call(
                 [&] {
@@ -108,7 +108,8 @@ int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, in
 extern "C" {
 
 int tb_ntt_set_variant(int forward, int log_block, int variant) {
-    if (log_block < 1 || log_block > tb::MAX_LOGB || variant < 0 || variant > 1 || (variant && log_block < 12))
+    if (log_block < 1 || log_block > tb::MAX_LOGB || variant < 0 || variant >= tb::NTT_VARIANTS ||
+        (variant && log_block < 12))
         return tb::set_error(TB_ERR_INVALID_ARGUMENT, "no such NTT variant");
     tb::g_variant[forward ? 1 : 0][log_block].store(variant);
     return TB_OK;

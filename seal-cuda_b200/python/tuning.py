@@ -31,7 +31,7 @@ def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
     "default_ms"}."""
     import torch
 
-    variants = (0, 1) if 12 <= logn <= 14 else (0,)
+    variants = (0, 1, 2) if 12 <= logn <= 14 else (0,)
     results = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for fwd, inv, budget in itertools.product(variants, variants, budgets):
