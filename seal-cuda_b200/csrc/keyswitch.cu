@@ -332,7 +332,7 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
     if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
     if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
-    if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 16384");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 32768");
     if (!target || !ct || keys.count < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     for (int g = 0; g < keys.count; g++)
         if (!keys.key[g]) return set_error(TB_ERR_NO_KEY, "missing key-switching key");
@@ -634,7 +634,7 @@ int relinearize_noalloc(const Context &c, int L, uint64_t *ct3, uint64_t cstride
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
     if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
     if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
-    if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 16384");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 32768");
     if (!ct3 || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     if (B == 0) return TB_OK;
     const uint64_t n = c.n;

@@ -358,7 +358,7 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     if (!ostride) ostride = 3ull * L * n;
     if (c.scheme == SCHEME_CKKS) return tensor_product_mods(c, c.d_mods, L, a, astride, b, bstride, out, ostride, B, s);
     if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV) return set_error(TB_ERR_UNSUPPORTED, "scheme has no multiply");
-    if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 16384");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 32768");
     ensure_pool_retains(c.device);
     const int logn = c.logn;
     cudaError_t e;

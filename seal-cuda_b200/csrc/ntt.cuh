@@ -19,6 +19,8 @@
 // rescaling steps fuse into the transform instead of running as extra passes.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace tb {
@@ -258,6 +260,97 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op
     else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
 }
 
+// ---------------------------------------------------------------- two-CTA limbs
+// A limb of 2^(LOGB+1) coefficients transformed by a cluster of two CTAs, each holding
+// one half in shared memory. The stage whose butterflies join the halves (the first
+// forward / last inverse stage, twiddle index 1 / the N^-1-scaled pair) reads and
+// writes the partner CTA's half through distributed shared memory between two
+// cluster barriers; every other stage runs inside one half exactly as the sub-block
+// passes of the split transform (sub-block = cluster rank). One launch, the same
+// arithmetic and order as the split transform, and the Op's load / store see whole-
+// limb coefficient indices, so every fused operation works at this length unchanged.
+template <int LOGB, class Op>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+    ntt_fwd_pair_kernel(Op op) {
+    namespace cg = cooperative_groups;
+    extern __shared__ uint64_t sm[];
+    constexpr int NB = 1 << LOGB;
+    constexpr int T = NttCfg<LOGB, 0>::THREADS;
+    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned half = cl.block_rank();
+    auto c = op.ctx((int)(blockIdx.x >> 1));
+    c.lm.sb = half;
+    const int off = (int)half << LOGB;
+    for (int e = threadIdx.x; e < NB; e += T) sm[swz(e)] = op.load(c, e + off);
+    cl.sync();
+    {
+        uint64_t *lo = cl.map_shared_rank(sm, 0u), *hi = cl.map_shared_rank(sm, 1u);
+        const uint64_t q = c.lm.q, q2 = q << 1;
+        const ulonglong2 w = __ldg(c.lm.roots + 1);
+        for (int j = (int)half * (NB / 2) + threadIdx.x; j < (int)(half + 1) * (NB / 2); j += T) {
+            const int p = swz(j);
+            uint64_t x = lo[p], y = hi[p];
+            ct_butterfly(x, y, w, q, q2);
+            lo[p] = x;
+            hi[p] = y;
+        }
+    }
+    cl.sync();
+    const uint32_t rbase = 2u + half;   // global stage 1 onwards, sub-block = half
+    constexpr int FIRST = REM != 0 ? REM : 3;
+    fwd_pass<FIRST, false, LOGB, T, 0, false>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
+    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
+        const int p = swz(e);
+        const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
+        if (p & 1) op.store2(c, e + off, w.y, w.x);
+        else op.store2(c, e + off, w.x, w.y);
+    }
+}
+
+template <int LOGB, class Op>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+    ntt_inv_pair_kernel(Op op) {
+    namespace cg = cooperative_groups;
+    extern __shared__ uint64_t sm[];
+    constexpr int NB = 1 << LOGB;
+    constexpr int T = NttCfg<LOGB, 0>::THREADS;
+    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned half = cl.block_rank();
+    auto c = op.ctx((int)(blockIdx.x >> 1));
+    c.lm.sb = half;
+    const int off = (int)half << LOGB;
+    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
+        uint64_t a, b;
+        op.load2(c, e + off, a, b);
+        const int p = swz(e);
+        *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
+    }
+    __syncthreads();
+    constexpr int LAST = REM ? REM : 3;
+    constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;
+    inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, LOGB + 1);
+    inv_pass<LAST, false, false, LOGB, T, 3 * PASSES, false>(op, c, sm, LOGB + 1);
+    cl.sync();
+    {
+        uint64_t *lo = cl.map_shared_rank(sm, 0u), *hi = cl.map_shared_rank(sm, 1u);
+        const uint64_t q = c.lm.q, q2 = q << 1;
+        for (int j = (int)half * (NB / 2) + threadIdx.x; j < (int)(half + 1) * (NB / 2); j += T) {
+            const int p = swz(j);
+            const uint64_t x = lo[p], y = hi[p];
+            const uint64_t u = x >= q2 ? x - q2 : x;
+            uint64_t sum = u + y;
+            sum = sum >= q2 ? sum - q2 : sum;
+            lo[p] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
+            hi[p] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
+        }
+    }
+    cl.sync();
+    for (int e = threadIdx.x; e < NB; e += T) op.store(c, e + off, sm[swz(e)]);
+}
+
 template <int LOGB>
 inline size_t ntt_smem_bytes() {
     return sizeof(uint64_t) * (size_t)(1 << LOGB);
@@ -277,6 +370,7 @@ __device__ __forceinline__ NttLimb make_limb(const Mod &m, uint32_t sb) {
 }
 
 constexpr int MAX_LOGB = 14;  // 16384 coefficients = 128 KB of shared memory per CTA
+constexpr int MAX_FUSED_LOGN = MAX_LOGB + 1;  // longest limb of the fused operations (a CTA pair)
 
 template <int LOGB, int V, class Op>
 inline cudaError_t launch_fwd(const Op &op, unsigned blocks, int s0, cudaStream_t s) {
@@ -306,6 +400,22 @@ inline cudaError_t launch_inv(const Op &op, unsigned blocks, int logn, int scale
 // the tuner (tune.cu), read at every launch.
 int ntt_variant(bool fwd, int logb);
 
+// Whole limbs of 2^(MAX_LOGB+1) coefficients, one CTA pair each (forward from stage 0,
+// inverse with the N^-1 scaling).
+template <bool FWD, class Op>
+inline cudaError_t launch_pair(const Op &op, unsigned blocks, cudaStream_t s) {
+    if (blocks > 0x3fffffffu) return cudaErrorInvalidValue;
+    const size_t smem = ntt_smem_bytes<MAX_LOGB>();
+    auto k = [] {
+        if constexpr (FWD) return ntt_fwd_pair_kernel<MAX_LOGB, Op>;
+        else return ntt_inv_pair_kernel<MAX_LOGB, Op>;
+    }();
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<2 * blocks, NttCfg<MAX_LOGB, 0>::THREADS, smem, s>>>(op);
+    return cudaGetLastError();
+}
+
 template <bool FWD, int LOGB, int V, class Op>
 inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
     if constexpr (FWD) return launch_fwd<LOGB, V>(op, blocks, s0_or_logn, s);
@@ -313,7 +423,8 @@ inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int
 }
 
 // Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry variants
-// with half and a quarter of the threads.
+// with half and a quarter of the threads. 15: whole 2^15 limbs on CTA pairs (forward
+// from stage 0 only, inverse with the scaling only).
 template <bool FWD, class Op>
 cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
 #define TB_CASE(B) \
@@ -332,6 +443,9 @@ cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn
     switch (logb) {
         TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
         TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE2(12) TB_CASE2(13) TB_CASE2(14)
+    case MAX_FUSED_LOGN:
+        if (FWD ? s0_or_logn != 0 : (s0_or_logn != MAX_FUSED_LOGN || !scale_last)) return cudaErrorInvalidValue;
+        return launch_pair<FWD>(op, blocks, s);
     default:
         return cudaErrorInvalidValue;
     }

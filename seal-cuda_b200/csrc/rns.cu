@@ -198,7 +198,7 @@ int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, 
     const uint64_t P = B * size;
     cudaError_t e;
     if (c.scheme == SCHEME_CKKS) {
-        if (c.logn > MAX_LOGB) return set_error(TB_ERR_UNSUPPORTED, "fused rescale supports N <= 16384");
+        if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused rescale supports N <= 32768");
         ensure_pool_retains(c.device);
         uint64_t *r = nullptr;
         e = cudaMallocAsync(&r, P * n * 8, s);
