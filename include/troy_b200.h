@@ -232,6 +232,14 @@ int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t 
                          uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride,
                          uint64_t batch, void *stream);
 /*
+ * The second polynomial ([L][n]) of a seed-compressed ciphertext, regenerated as the
+ * reference's GPU loader does (CiphertextCuda::load with a context,
+ * src/ciphertext_cuda.cu:157-183): one cuRAND state per coefficient g seeded with
+ * g + seed, limb j = (uint64) (curand_uniform_double * q_j); inverse_ntt != 0 (BFV)
+ * then takes it out of the NTT domain. seed must be non-zero.
+ */
+int tb_expand_seeded(tb_context *ctx, int L, uint64_t seed, int inverse_ntt, uint64_t *c1, void *stream);
+/*
  * Decrypts `batch` ciphertexts of `size` polynomials at level L (DecryptorCuda::decrypt,
  * src/decryptor_cuda.cu:92-328): BFV scale-and-round / BGV exact conversion (times
  * correction^-1) give n words mod t per plaintext; CKKS gives [L][n] in NTT form.

@@ -8,7 +8,9 @@
 
 #include <cmath>
 #include <complex>
+#include <cstring>
 #include <random>
+#include <sstream>
 #include <vector>
 
 #include "troy_cuda.cuh"
@@ -84,6 +86,58 @@ extern "C" int ref_gpu_ckks_chain(size_t n, const uint64_t *moduli, int count, i
             err = std::max(err, std::abs(got[i] - v[j] * w[j]));
         }
         *max_err = err;
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    } catch (...) {
+        return 1;
+    }
+}
+
+// The reference GPU path's symmetric encryption of a batch-encoded (BFV, `values`) or
+// CKKS-encoded (`reals`, at `scale`) plaintext under a seeded Blake2xb factory: its
+// seed-compressed wire bytes (save) and the words its own loader (load with a
+// context) expands them to. bytes: cap bytes, *len written; words: 2 * L * n.
+extern "C" int ref_gpu_seeded_ct(int scheme, size_t n, const uint64_t *moduli, int count, uint64_t t,
+                                 const uint64_t *seed8, const uint64_t *values, const double *reals, size_t nvalues,
+                                 double scale, char *bytes, size_t cap, size_t *len, uint64_t *words, uint64_t *seed_out) {
+    try {
+        KernelProvider::initialize();
+        troy::EncryptionParameters host((SchemeType)scheme);
+        host.setPolyModulusDegree(n);
+        std::vector<Modulus> q;
+        for (int i = 0; i < count; i++) q.emplace_back(moduli[i]);
+        host.setCoeffModulus(q);
+        if ((SchemeType)scheme != SchemeType::ckks) host.setPlainModulus(Modulus(t));
+        troy::PRNGSeed seed;
+        std::copy_n(seed8, 8, seed.begin());
+        host.setRandomGenerator(std::make_shared<troy::Blake2xbPRNGFactory>(seed));
+        EncryptionParameters parms(host);
+        SEALContext context(parms, true, SecurityLevel::none);
+        KeyGenerator keygen(context);
+        Encryptor encryptor(context, keygen.secretKey());
+        Plaintext p;
+        if ((SchemeType)scheme == SchemeType::ckks) {
+            CKKSEncoder encoder(context);
+            std::vector<std::complex<double>> v(nvalues);
+            for (size_t i = 0; i < nvalues; i++) v[i] = {reals[i], 0.0};
+            encoder.encode(v, scale, p);
+        } else {
+            BatchEncoder encoder(context);
+            std::vector<uint64_t> v(values, values + nvalues);
+            encoder.encode(v, p);
+        }
+        Ciphertext c = encryptor.encryptSymmetric(p);
+        *seed_out = c.seed();
+        std::ostringstream os;
+        c.save(os);
+        const std::string b = os.str();
+        if (b.size() > cap) return 3;
+        std::memcpy(bytes, b.data(), b.size());
+        *len = b.size();
+        Ciphertext back;
+        std::istringstream is(b);
+        back.load(is, context);
+        const size_t w = back.size() * back.coeffModulusSize() * back.polyModulusDegree();
+        cudaMemcpy(words, back.data().get(), w * 8, cudaMemcpyDeviceToHost);
         return cudaGetLastError() == cudaSuccess ? 0 : 2;
     } catch (...) {
         return 1;

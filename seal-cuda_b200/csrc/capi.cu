@@ -38,6 +38,7 @@ int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int
                       cudaStream_t s);
 int decrypt(Context &c, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t cstride, uint64_t *out,
             uint64_t ostride, uint64_t correction, uint64_t B, cudaStream_t s);
+int expand_seeded(Context &c, int L, uint64_t seed, bool inverse_ntt, uint64_t *c1, cudaStream_t s);
 int batch_encode(Context &c, const uint64_t *slots, uint64_t sstride, uint32_t count, uint64_t *out, uint64_t B,
                  cudaStream_t s);
 int batch_decode(Context &c, const uint64_t *plain, uint64_t *slots, uint64_t sstride, uint64_t B, cudaStream_t s);
@@ -269,6 +270,10 @@ int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t 
         return tb::encrypt_symmetric(c, seed8, sk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch,
                                      S(stream));
     });
+}
+
+int tb_expand_seeded(tb_context *ctx, int L, uint64_t seed, int inverse_ntt, uint64_t *c1, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::expand_seeded(c, L, seed, inverse_ntt != 0, c1, S(stream)); });
 }
 
 int tb_decrypt(tb_context *ctx, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t ct_stride,

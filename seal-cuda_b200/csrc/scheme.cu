@@ -5,6 +5,8 @@
 // (src/utils/rlwe.cpp:152-357, src/keygenerator.cpp:47-329,
 // src/encryptor.cpp:92-237), so with a seeded factory the ciphertext and key words
 // are identical to the reference's CPU path.
+#include <curand_kernel.h>
+
 #include <algorithm>
 #include <mutex>
 #include <vector>
@@ -534,6 +536,32 @@ int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int
                                                                       count);
     }
     return status_from(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------ seeded ciphertexts
+
+// The second polynomial of a seed-compressed ciphertext as the reference's GPU loader
+// regenerates it (CiphertextCuda::load, src/ciphertext_cuda.cu:157-183, with
+// sampler::setupCurandStates / kSamplePolyUniform, src/utils/rlwe_cuda.cu:25-28,
+// 136-151): coefficient g takes a cuRAND XORWOW state initialised with seed g + seed,
+// subsequence 0, offset 0, and limb j takes (uint64) (uniform double * q_j). The
+// values come from cuRAND itself, called here exactly as there.
+__global__ void seeded_uniform_kernel(uint64_t *c1, const Mod *__restrict__ mods, int L, uint32_t n, uint64_t seed) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    curandState st;
+    curand_init((unsigned long long)g + seed, 0ull, 0ull, &st);
+    for (int j = 0; j < L; j++) c1[g + (size_t)j * n] = (uint64_t)(curand_uniform_double(&st) * (double)mods[j].value);
+}
+
+int expand_seeded(Context &c, int L, uint64_t seed, bool inverse_ntt, uint64_t *c1, cudaStream_t s) {
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    if (!c1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (!seed) return set_error(TB_ERR_INVALID_ARGUMENT, "seed is zero");
+    seeded_uniform_kernel<<<grid_for(c.n, 256), 256, 0, s>>>(c1, c.d_mods, L, (uint32_t)c.n, seed);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && inverse_ntt) e = transform<false>(c, c1, 1, 0, L, false, s);
+    return status_from(e);
 }
 
 // ------------------------------------------------------------------ decryption

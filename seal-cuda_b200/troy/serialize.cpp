@@ -7,6 +7,7 @@
 #include <istream>
 #include <ostream>
 
+#include "device_util.hpp"
 #include "troy_b200.hpp"
 
 namespace troyn {
@@ -116,11 +117,32 @@ void Ciphertext::load(std::istream &s) {
     data_.fromHost(w.data(), w.size());
 }
 
+// With a context, a seed-compressed ciphertext (seed != 0: only c0 on the wire) is
+// expanded: c1 regenerated from the seed as the reference's GPU loader does
+// (src/ciphertext_cuda.cu:137-184), inverse-transformed for BFV.
 void Ciphertext::load(std::istream &s, const SEALContext &context) {
-    load(s);
+    bool terms;
+    std::uint64_t seed;
+    loadHeader(s, terms, seed);
+    if (terms) throw std::invalid_argument("Trying to load a termed ciphertext, but indices is not specified");
     auto d = context.getContextData(parms_id_);
     if (!d || (std::size_t)d->levelLimbs() != limbs_ || context.polyModulusDegree() != n_)
         throw std::invalid_argument("ciphertext is not valid for encryption parameters");
+    const auto words = get<std::size_t>(s);
+    if (seed == 0) {
+        if (words != size_ * n_ * limbs_) throw std::invalid_argument("ciphertext data size mismatch");
+        auto w = get_words(s, words);
+        data_.fromHost(w.data(), w.size());
+        return;
+    }
+    if (size_ > 2) throw std::invalid_argument("Seed exists but size is not 2.");
+    if (words != n_ * limbs_) throw std::invalid_argument("ciphertext data size mismatch");
+    auto w = get_words(s, words);
+    size_ = 2;
+    data_.fromHost(w.data(), w.size());
+    data_.resize(2 * n_ * limbs_);
+    detail::tb_ok(tb_expand_seeded(context.handle(), (int)limbs_, seed, context.scheme() == SchemeType::bfv,
+                                   data_.get() + n_ * limbs_, nullptr));
 }
 
 // Only the listed coefficients of c0 travel (in coefficient form), then the remaining
