@@ -116,6 +116,15 @@ int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint
  */
 int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b, uint64_t b_stride,
                 uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
+/*
+ * One product of a size-a_size and a size-b_size ciphertext (2 .. 64 polynomials each,
+ * packed [size][L][n]) at level L into a_size + b_size - 1 polynomials at out: the
+ * reference's bfvMultiply / bgvMultiply / ckksMultiply for any operand sizes
+ * (src/evaluator_cuda.cu:283-501), e.g. an unrelinearized product times another
+ * ciphertext. out must not overlap the inputs.
+ */
+int tb_multiply_sizes(tb_context *ctx, int L, const uint64_t *a, int a_size, const uint64_t *b, int b_size,
+                      uint64_t *out, void *stream);
 
 /* ------------------------------------------------------------ key switching */
 

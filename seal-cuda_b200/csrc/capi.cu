@@ -14,6 +14,8 @@ int dyadic_product(const Context &c, const uint64_t *a, const uint64_t *b, uint6
                    int limbs, cudaStream_t s);
 int tensor_product(const Context &c, int first, int L, const uint64_t *a, uint64_t astride, const uint64_t *b,
                    uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
+int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uint64_t *b, int sb, uint64_t *out,
+                   cudaStream_t s);
 int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const uint64_t *b, uint64_t bstride,
              uint64_t *out, uint64_t ostride, uint64_t B, cudaStream_t s);
 int keyswitch(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct, uint64_t cstride,
@@ -180,6 +182,11 @@ int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, co
     return on_device(ctx, [&](tb::Context &c) {
         return tb::multiply(c, L, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
     });
+}
+
+int tb_multiply_sizes(tb_context *ctx, int L, const uint64_t *a, int a_size, const uint64_t *b, int b_size,
+                      uint64_t *out, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) { return tb::multiply_sizes(c, L, a, a_size, b, b_size, out, S(stream)); });
 }
 
 int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target_stride, uint64_t *ct,

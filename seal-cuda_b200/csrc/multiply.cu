@@ -435,4 +435,113 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     return e == cudaSuccess ? TB_OK : status_from(e);
 }
 
+// ---------------------------------------------------------- any operand sizes
+
+// out[k] = sum_{i+j=k} x[i] (.) y[j] over `limbs` limbs (mods[l]) for sa x sb polynomials
+// (packed [sa][limbs][N] and [sb][limbs][N]); canonical outputs, the exact residues of
+// the reference's dyadic products and additions (any input below 2^64).
+__global__ void tensor_sizes_kernel(const uint64_t *__restrict__ x, int sa, const uint64_t *__restrict__ y, int sb,
+                                    uint64_t *__restrict__ out, const Mod *__restrict__ mods, int limbs, int logn) {
+    const uint64_t per = (uint64_t)limbs << logn;
+    const uint64_t total = (uint64_t)(sa + sb - 1) * per;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(w / per);
+        const uint64_t r = w - (uint64_t)k * per;
+        const Mod m = mods[r >> logn];
+        uint64_t acc = 0;
+        for (int i = k < sb ? 0 : k - sb + 1; i <= k && i < sa; i++)
+            acc = add_mod(acc, mul_mod(x[(uint64_t)i * per + r], y[(uint64_t)(k - i) * per + r], m), m.value);
+        out[w] = acc;
+    }
+}
+
+// One product of a size-sa and a size-sb ciphertext at level L into sa + sb - 1
+// polynomials (bfvMultiply / bgvMultiply / ckksMultiply for any sizes,
+// src/evaluator_cuda.cu:283-501): the same steps as the batched size-2 path, on
+// packed copies of the operands, with the general tensor.
+int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uint64_t *b, int sb, uint64_t *out,
+                   cudaStream_t s) {
+    const int K = (int)c.chain.size();
+    if (L < 1 || L > K) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    if (!a || !b || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (sa < 2 || sb < 2 || sa > 64 || sb > 64) return set_error(TB_ERR_INVALID_ARGUMENT, "ciphertext sizes must be 2 .. 64");
+    if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV && c.scheme != SCHEME_CKKS)
+        return set_error(TB_ERR_UNSUPPORTED, "scheme has no multiply");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 32768");
+    const int logn = c.logn;
+    const uint64_t n = c.n, pq = (uint64_t)L * n;
+    const int P = sa + sb, D = sa + sb - 1;
+    if (c.scheme == SCHEME_CKKS) {
+        TraceScope ts("tensor", s);
+        tensor_sizes_kernel<<<grid_for((uint64_t)D * pq, 256), 256, 0, s>>>(a, sa, b, sb, out, c.d_mods, L, logn);
+        return status_from(cudaGetLastError());
+    }
+    ensure_pool_retains(c.device);
+    ScratchBuf buf(s);
+    cudaError_t e;
+    if (c.scheme == SCHEME_BGV) {
+        e = cudaMallocAsync(&buf.p, (uint64_t)(P + D) * pq * 8, s);
+        if (e != cudaSuccess) return status_from(e);
+        uint64_t *x = (uint64_t *)buf.p, *t = x + (uint64_t)P * pq;
+        e = cudaMemcpyAsync(x, a, sa * pq * 8, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(x + sa * pq, b, sb * pq * 8, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return status_from(e);
+        PackedNttOp<true> f{x, x, c.d_mods, L, logn};
+        e = dispatch_ntt<true>(logn, f, (unsigned)(P * L), 0, 0, s);
+        if (e != cudaSuccess) return status_from(e);
+        tensor_sizes_kernel<<<grid_for((uint64_t)D * pq, 256), 256, 0, s>>>(x, sa, x + sa * pq, sb, t, c.d_mods, L,
+                                                                           logn);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return status_from(e);
+        CtInttOutOp oi{t, out, (uint64_t)D * pq, c.d_mods, D, L, logn};
+        e = dispatch_ntt<false>(logn, oi, (unsigned)(D * L), logn, 1, s);
+        return status_from(e);
+    }
+    // BFV
+    const RnsLevel &lv = c.levels[L];
+    if (!lv.d_consts) return set_error(TB_ERR_UNSUPPORTED, "plain modulus not coprime to the coefficient moduli");
+    if (L > MAXL) return set_error(TB_ERR_UNSUPPORTED, "BFV multiply supports at most 32 data limbs");
+    const int bsk = lv.bsk;
+    const uint64_t pb = (uint64_t)bsk * n;
+    e = cudaMallocAsync(&buf.p, ((uint64_t)P * (2 * pq + pb) + (uint64_t)D * (pq + pb)) * 8, s);
+    if (e != cudaSuccess) return status_from(e);
+    uint64_t *x0 = (uint64_t *)buf.p;          // [P][L][N] operands, coefficient form
+    uint64_t *xq = x0 + (uint64_t)P * pq;      // [P][L][N] NTT in q
+    uint64_t *xb = xq + (uint64_t)P * pq;      // [P][bsk][N] lifted to Bsk, NTT
+    uint64_t *tq = xb + (uint64_t)P * pb;      // [D][L][N]
+    uint64_t *tbk = tq + (uint64_t)D * pq;     // [D][bsk][N]
+    e = cudaMemcpyAsync(x0, a, sa * pq * 8, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x0 + sa * pq, b, sb * pq * 8, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return status_from(e);
+    PackedNttOp<true> fq{x0, xq, c.d_mods, L, logn};
+    e = dispatch_ntt<true>(logn, fq, (unsigned)(P * L), 0, 0, s);
+    if (e != cudaSuccess) return status_from(e);
+    // the lift reads polynomial p of four-polynomial groups: with both strides 4 L N
+    // and b starting two polynomials in, polynomial p of x0 for every p
+    behz_lift_kernel<<<grid_for((uint64_t)P * n, 256), 256, 0, s>>>(x0, 4 * pq, x0 + 2 * pq, 4 * pq, xb, c.d_mods,
+                                                                   lv.d_bsk_mods, lv.d_consts, lv.off, L, bsk, logn,
+                                                                   (uint64_t)P);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return status_from(e);
+    PackedNttOp<true> fb{xb, xb, lv.d_bsk_mods, bsk, logn};
+    e = dispatch_ntt<true>(logn, fb, (unsigned)(P * bsk), 0, 0, s);
+    if (e != cudaSuccess) return status_from(e);
+    tensor_sizes_kernel<<<grid_for((uint64_t)D * pq, 256), 256, 0, s>>>(xq, sa, xq + sa * pq, sb, tq, c.d_mods, L, logn);
+    tensor_sizes_kernel<<<grid_for((uint64_t)D * pb, 256), 256, 0, s>>>(xb, sa, xb + sa * pb, sb, tbk, lv.d_bsk_mods,
+                                                                       bsk, logn);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return status_from(e);
+    PackedNttOp<false> iq{tq, tq, c.d_mods, L, logn};
+    e = dispatch_ntt<false>(logn, iq, (unsigned)(D * L), logn, 1, s);
+    if (e != cudaSuccess) return status_from(e);
+    PackedNttOp<false> ib{tbk, tbk, lv.d_bsk_mods, bsk, logn};
+    e = dispatch_ntt<false>(logn, ib, (unsigned)(D * bsk), logn, 1, s);
+    if (e != cudaSuccess) return status_from(e);
+    // the floor reads polynomial p = ct * 3 + poly: ostride 3 L N maps it to out + p L N
+    behz_floor_sk_kernel<<<grid_for((uint64_t)D * n, 256), 256, 0, s>>>(tq, tbk, out, 3 * pq, c.d_mods, lv.d_bsk_mods,
+                                                                       lv.d_consts, lv.off, L, lv.bB, logn,
+                                                                       (uint64_t)D);
+    return status_from(cudaGetLastError());
+}
+
 }  // namespace tb

@@ -694,18 +694,22 @@ void Evaluator::addMany(const std::vector<Ciphertext> &cts, Ciphertext &d) const
 }
 
 // EvaluatorCuda::multiplyInplace -> bfvMultiply / ckksMultiply / bgvMultiply
-// (src/evaluator_cuda.cu:262-501); operands of size 2 (the library's fused tensor).
+// (src/evaluator_cuda.cu:262-501): size-2 operands take the fused batched product,
+// larger ones the general-size product (size a + size b - 1 polynomials).
 void Evaluator::multiplyInplace(Ciphertext &a, const Ciphertext &b) const {
     const auto &d = data_of(context_, a);
     if (a.parmsID() != b.parmsID()) throw std::invalid_argument("encrypted1 and encrypted2 parameter mismatch");
     check_form(context_, a);
     check_form(context_, b);
-    if (a.size() != 2 || b.size() != 2)
-        throw std::invalid_argument("multiply takes ciphertexts of size 2 (relinearize first)");
+    if (a.size() < 2 || b.size() < 2) throw std::invalid_argument("encrypted is empty");
     const int L = d.levelLimbs();
     Ciphertext out;
-    out.resize(context_, a.parmsID(), 3);
-    check(tb_multiply(context_.handle(), L, a.data(), 0, b.data(), 0, out.data(), 0, 1, nullptr));
+    out.resize(context_, a.parmsID(), a.size() + b.size() - 1);
+    if (a.size() == 2 && b.size() == 2)
+        check(tb_multiply(context_.handle(), L, a.data(), 0, b.data(), 0, out.data(), 0, 1, nullptr));
+    else
+        check(tb_multiply_sizes(context_.handle(), L, a.data(), (int)a.size(), b.data(), (int)b.size(), out.data(),
+                                nullptr));
     out.isNttForm() = a.isNttForm();
     out.scale() = a.scale();
     out.correctionFactor() = a.correctionFactor();
