@@ -84,6 +84,7 @@ class Oracle:
             bind("ntt_inverse_rns", _c.c_int, [_c.c_int, _u64, _c.c_int, _u64, _c.c_int])
         if kind == "ref":
             bind("parms_id", _c.c_int, [_c.c_int, _sz, _u64, _c.c_int, _c.c_uint64, _u64])
+            bind("bfv_default", _c.c_int, [_sz, _c.c_int, _u64, _c.c_int])
 
     # ------------------------------------------------------------ primitives
     def ntt_tables(self, logn, q):
@@ -161,6 +162,13 @@ class Oracle:
         if self._f["parms_id"](scheme, n, _arr(moduli), len(moduli), t, out):
             raise ValueError("invalid parameters")
         return [int(x) for x in out]
+
+    def bfv_default(self, n, sec):
+        """CoeffModulus::BFVDefault of the compiled reference (kind "ref" only); sec is
+        128, 192 or 256. None when the reference rejects the arguments."""
+        out = np.zeros(64, np.uint64)
+        k = self._f["bfv_default"](n, sec, out, 64)
+        return None if k < 0 else [int(x) for x in out[:k]]
 
     def plain_modulus_batching(self, n, bits):
         out = np.zeros(1, np.uint64)

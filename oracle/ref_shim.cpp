@@ -141,6 +141,19 @@ int ref_parms_id(int scheme, size_t n, const uint64_t *moduli, int count, uint64
     }
 }
 
+// CoeffModulus::BFVDefault (src/modulus.cpp:53-78): the default primes of a degree and
+// security level (1 tc128, 2 tc192, 3 tc256); returns the count, -1 on error.
+int ref_bfv_default(size_t n, int sec, uint64_t *out, int cap) {
+    try {
+        auto v = CoeffModulus::BFVDefault(n, (SecurityLevel)sec);
+        if ((int)v.size() > cap) return -1;
+        for (size_t i = 0; i < v.size(); i++) out[i] = v[i].value();
+        return (int)v.size();
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_plain_modulus_batching(size_t n, int bits, uint64_t *out) {
     try {
         *out = PlainModulus::Batching(n, bits).value();

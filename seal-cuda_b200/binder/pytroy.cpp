@@ -86,6 +86,8 @@ PYBIND11_MODULE(pytroy, m) {
     py::class_<CoeffModulus>(m, "CoeffModulus")
         .def_static("max_bit_count", &CoeffModulus::MaxBitCount, py::arg("poly_modulus_degree"),
                     py::arg("sec_level") = SecurityLevel::tc128)
+        .def_static("bfv_default", &CoeffModulus::BFVDefault, py::arg("poly_modulus_degree"),
+                    py::arg("sec_level") = SecurityLevel::tc128)
         .def_static("create", py::overload_cast<std::size_t, vector<int>>(&CoeffModulus::Create))
         .def_static("create", py::overload_cast<std::size_t, const Modulus &, vector<int>>(&CoeffModulus::Create));
     py::class_<PlainModulus>(m, "PlainModulus")

@@ -186,6 +186,38 @@ int CoeffModulus::MaxBitCount(std::size_t n, SecurityLevel sec) {
     return it->second[sec == SecurityLevel::tc128 ? 0 : (sec == SecurityLevel::tc192 ? 1 : 2)];
 }
 
+// The default primes (the reference's util/globals.cpp tables): per degree and level,
+// groups of equal bit size, each the largest primes = 1 mod 2N of that size in
+// descending order; five single-prime entries are other primes of their size, listed.
+std::vector<Modulus> CoeffModulus::BFVDefault(std::size_t n, SecurityLevel sec) {
+    if (!MaxBitCount(n, sec)) throw std::invalid_argument("non-standard poly_modulus_degree");
+    if (sec == SecurityLevel::none) throw std::invalid_argument("invalid security level");
+    struct Group {
+        int bits, count;
+    };
+    static const std::map<std::pair<std::size_t, int>, std::vector<Group>> groups = {
+        {{1024, 128}, {{27, 1}}},   {{2048, 128}, {{54, 1}}},  {{4096, 128}, {{36, 2}, {37, 1}}},
+        {{8192, 128}, {{43, 2}, {44, 3}}}, {{16384, 128}, {{48, 3}, {49, 6}}}, {{32768, 128}, {{55, 15}, {56, 1}}},
+        {{1024, 192}, {{19, 1}}},   {{2048, 192}, {{37, 1}}},  {{4096, 192}, {{25, 3}}},
+        {{8192, 192}, {{38, 4}}},   {{16384, 192}, {{50, 6}}}, {{32768, 192}, {{54, 5}, {55, 6}}},
+        {{1024, 256}, {{14, 1}}},   {{2048, 256}, {{29, 1}}},  {{4096, 256}, {{58, 1}}},
+        {{8192, 256}, {{39, 2}, {40, 1}}}, {{16384, 256}, {{47, 3}, {48, 2}}}, {{32768, 256}, {{52, 1}, {53, 8}}}};
+    static const std::map<std::pair<std::size_t, int>, uint64_t> single = {
+        {{1024, 128}, 0x7e00001ull},           {{2048, 128}, 0x3fffffff000001ull}, {{2048, 192}, 0x1ffffc0001ull},
+        {{2048, 256}, 0x1ffc0001ull},          {{4096, 256}, 0x3ffffffff040001ull}};
+    const std::pair<std::size_t, int> key{n, (int)sec};
+    auto it = single.find(key);
+    if (it != single.end()) return {Modulus(it->second)};
+    std::vector<Modulus> out;
+    for (const Group &g : groups.at(key)) {
+        std::vector<uint64_t> primes;
+        if (!tb::host::get_primes(2 * (uint64_t)n, g.bits, (std::size_t)g.count, primes))
+            throw std::logic_error("failed to find enough qualifying primes");
+        for (uint64_t p : primes) out.emplace_back(p);   // largest first
+    }
+    return out;
+}
+
 Modulus PlainModulus::Batching(std::size_t n, int bit_size) { return CoeffModulus::Create(n, {bit_size})[0]; }
 std::vector<Modulus> PlainModulus::Batching(std::size_t n, std::vector<int> bit_sizes) {
     return CoeffModulus::Create(n, bit_sizes);

@@ -78,6 +78,10 @@ struct CoeffModulus {
                                        std::vector<int> bit_sizes);
     // CoeffModulus::MaxBitCount for the HE-standard security levels (src/modulus.h:427-440)
     static int MaxBitCount(std::size_t poly_modulus_degree, SecurityLevel sec_level = SecurityLevel::tc128);
+    // CoeffModulus::BFVDefault (src/modulus.cpp:53-78): the default primes of a standard
+    // degree at a security level
+    static std::vector<Modulus> BFVDefault(std::size_t poly_modulus_degree,
+                                           SecurityLevel sec_level = SecurityLevel::tc128);
 };
 
 struct PlainModulus {

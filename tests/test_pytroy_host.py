@@ -64,3 +64,19 @@ def test_invalid_parameters_are_reported_without_a_device():
     assert ctx.parameter_error_name() == "invalid_parameters_insecure"
     with pytest.raises(ValueError):
         pytroy.KeyGenerator(ctx)
+
+
+def test_bfv_default_primes_match_the_reference():
+    ref = Oracle("ref") if available("ref") else None
+    L = pytroy.SecurityLevel
+    for sec, bits in ((L.tc128, 128), (L.tc192, 192), (L.tc256, 256)):
+        for n in (1024, 2048, 4096, 8192, 16384, 32768):
+            got = [m.value() for m in pytroy.CoeffModulus.bfv_default(n, sec)]
+            assert sum(q.bit_length() for q in got) <= pytroy.CoeffModulus.max_bit_count(n, sec)
+            assert all(pytroy.Modulus(q).is_prime() and q % (2 * n) == 1 for q in got)
+            if ref is not None:
+                assert got == ref.bfv_default(n, bits), (n, bits)
+    with pytest.raises(ValueError):
+        pytroy.CoeffModulus.bfv_default(4096, L.none)
+    with pytest.raises(ValueError):
+        pytroy.CoeffModulus.bfv_default(3000)
