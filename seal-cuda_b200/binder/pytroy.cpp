@@ -6,6 +6,7 @@
 // registered after the regular one and so is never reached, and
 // rotate_rows(cipher, galois_keys) rotates the columns (binder.cu:682).
 #include <pybind11/complex.h>
+#include <pybind11/eval.h>
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -20,6 +21,34 @@ namespace py = pybind11;
 using namespace troyn;
 using std::complex;
 using std::vector;
+
+// ParmsID (std::array<uint64_t, 4>) crosses as pytroy.ParmsID, a list of the four
+// words with the reference binder's vec() (binder/binder.cu:186-194; there vec()
+// returns an empty list, here the words); any four-int sequence converts back.
+namespace pybind11 {
+namespace detail {
+template <>
+struct type_caster<troyn::ParmsID> {
+    PYBIND11_TYPE_CASTER(troyn::ParmsID, const_name("ParmsID"));
+    bool load(handle src, bool) {
+        if (!isinstance<sequence>(src) || isinstance<str>(src) || isinstance<bytes>(src)) return false;
+        auto seq = reinterpret_borrow<sequence>(src);
+        if (seq.size() != 4) return false;
+        for (size_t i = 0; i < 4; i++) {
+            make_caster<std::uint64_t> c;
+            if (!c.load(seq[i], true)) return false;
+            value[i] = cast_op<std::uint64_t>(c);
+        }
+        return true;
+    }
+    static handle cast(const troyn::ParmsID &v, return_value_policy, handle) {
+        list words;
+        for (auto x : v) words.append(int_(x));
+        return module_::import("pytroy").attr("ParmsID")(words).release();
+    }
+};
+}  // namespace detail
+}  // namespace pybind11
 
 namespace {
 
@@ -94,8 +123,15 @@ PYBIND11_MODULE(pytroy, m) {
         .def_static("batching", py::overload_cast<std::size_t, int>(&PlainModulus::Batching))
         .def_static("batching", py::overload_cast<std::size_t, vector<int>>(&PlainModulus::Batching));
 
-    // ParmsID (std::array<uint64_t, 4>) crosses as a list of four ints through
-    // pybind11's STL casters, as in the reference module.
+    // pytroy.ParmsID: the parms_id words as a list, with vec() (see the caster above).
+    py::exec(R"(
+class ParmsID(list):
+    """A parms_id: the four 64-bit words of its BLAKE2b hash."""
+
+    def vec(self):
+        return list(self)
+)",
+             m.attr("__dict__"));
 
     py::class_<Blake2xbPRNGFactory, std::shared_ptr<Blake2xbPRNGFactory>>(m, "Blake2xbPRNGFactory")
         .def(py::init<>())
@@ -168,6 +204,7 @@ PYBIND11_MODULE(pytroy, m) {
         .def(py::init<const SEALContext &, ParmsID, std::size_t>())
         .def("correction_factor", py::overload_cast<>(&Ciphertext::correctionFactor, py::const_))
         .def("set_correction_factor", [](Ciphertext &self, uint64_t c) { self.correctionFactor() = c; })
+        .def("resize", py::overload_cast<std::size_t>(&Ciphertext::resize))
         .def("reserve", &Ciphertext::reserve)
         .def("parms_id", py::overload_cast<>(&Ciphertext::parmsID, py::const_))
         .def("set_parms_id", [](Ciphertext &self, const ParmsID &p) { self.parmsID() = p; })

@@ -227,6 +227,13 @@ public:
     }
     void resize(const SEALContext &context, const ParmsID &parms_id, std::size_t size);
     void resize(const SEALContext &context, std::size_t size) { resize(context, parms_id_, size); }
+    // same degree and limb count, `size` polynomials (CiphertextCuda::resize(size_t),
+    // src/ciphertext_cuda.cuh:83-88): the common prefix kept, new polynomials zero
+    void resize(std::size_t size) {
+        if ((size < 2 && size != 0) || size > 16) throw std::invalid_argument("invalid size");
+        data_.resize(size * limbs_ * n_);
+        size_ = size;
+    }
     void reserve(std::size_t) {}
     std::size_t size() const { return size_; }
     std::size_t coeffModulusSize() const { return limbs_; }
