@@ -85,6 +85,7 @@ class Oracle:
         if kind == "ref":
             bind("parms_id", _c.c_int, [_c.c_int, _sz, _u64, _c.c_int, _c.c_uint64, _u64])
             bind("bfv_default", _c.c_int, [_sz, _c.c_int, _u64, _c.c_int])
+            bind("context_consts", _c.c_int, [_c.c_int, _sz, _u64, _c.c_int, _c.c_uint64, _c.c_int, _u64])
 
     # ------------------------------------------------------------ primitives
     def ntt_tables(self, logn, q):
@@ -169,6 +170,23 @@ class Oracle:
         out = np.zeros(64, np.uint64)
         k = self._f["bfv_default"](n, sec, out, 64)
         return None if k < 0 else [int(x) for x in out[:k]]
+
+    def context_consts(self, scheme, n, moduli, t, sec):
+        """The reference's first-level qualifiers and constants (kind "ref" only), as a
+        dict; None when the reference throws."""
+        out = np.zeros(9 + 6 * len(moduli), np.uint64)
+        L = self._f["context_consts"](scheme, n, _arr(moduli), len(moduli), t, sec, out)
+        if L < 0:
+            return None
+        head = [int(x) for x in out[:9]]
+        rows = out[9:9 + 6 * L].reshape(6, L)
+        keys = ("total", "delta", "delta_quotient", "upper_half_increment", "plain_upper_half_increment",
+                "upper_half_threshold")
+        d = {k: [int(x) for x in r] for k, r in zip(keys, rows)}
+        d.update(error=np.int64(np.uint64(head[0])).item(), using_fft=head[1], using_ntt=head[2],
+                 using_batching=head[3], using_fast_plain_lift=head[4], using_descending_modulus_chain=head[5],
+                 sec_level=head[6], q_mod_t=head[7], plain_upper_half_threshold=head[8])
+        return d
 
     def plain_modulus_batching(self, n, bits):
         out = np.zeros(1, np.uint64)

@@ -154,6 +154,48 @@ int ref_bfv_default(size_t n, int sec, uint64_t *out, int cap) {
     }
 }
 
+// The first data level's qualifiers and precomputed constants
+// (SEALContext::ContextData, src/context.h): out = [error, using_fft, using_ntt,
+// using_batching, using_fast_plain_lift, using_descending_modulus_chain, sec_level,
+// q_mod_t, plain_threshold, then L words each of: total modulus, delta operands,
+// delta quotients, upper-half increment, plain upper-half increment, upper-half
+// threshold]; returns L, or -1.
+int ref_context_consts(int scheme, size_t n, const uint64_t *moduli, int count, uint64_t t, int sec, uint64_t *out) {
+    try {
+        EncryptionParameters parms((SchemeType)scheme);
+        parms.setPolyModulusDegree(n);
+        std::vector<Modulus> mods;
+        for (int i = 0; i < count; i++) mods.emplace_back(moduli[i]);
+        parms.setCoeffModulus(mods);
+        if (scheme != 2) parms.setPlainModulus(Modulus(t));
+        SEALContext context(parms, true, (SecurityLevel)sec);
+        auto d = context.firstContextData();
+        const auto q = d->qualifiers();
+        const size_t L = d->parms().coeffModulus().size();
+        size_t k = 0;
+        out[k++] = (uint64_t)(int64_t)q.parameter_error;
+        out[k++] = q.using_fft;
+        out[k++] = q.using_ntt;
+        out[k++] = q.using_batching;
+        out[k++] = q.using_fast_plain_lift;
+        out[k++] = q.using_descending_modulus_chain;
+        out[k++] = (uint64_t)(int)q.sec_level;
+        const bool ok = q.parametersSet();
+        const bool ckks = scheme == 2;
+        out[k++] = ok && !ckks ? d->coeffModulusModPlainModulus() : 0;
+        out[k++] = ok ? d->plainUpperHalfThreshold() : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok ? d->totalCoeffModulus()[i] : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok && !ckks ? d->coeffDivPlainModulus()[i].operand : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok && !ckks ? d->coeffDivPlainModulus()[i].quotient : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok && !ckks ? d->upperHalfIncrement()[i] : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok ? d->plainUpperHalfIncrement()[i] : 0;
+        for (size_t i = 0; i < L; i++) out[k++] = ok && ckks ? d->upperHalfThreshold()[i] : 0;
+        return (int)L;
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_plain_modulus_batching(size_t n, int bits, uint64_t *out) {
     try {
         *out = PlainModulus::Batching(n, bits).value();

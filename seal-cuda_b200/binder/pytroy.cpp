@@ -162,10 +162,64 @@ class ParmsID(list):
 
     using CD = SEALContext::ContextData;
     auto cd = [](std::shared_ptr<const CD> p) { return std::const_pointer_cast<CD>(p); };
+    using Q = EncryptionParameterQualifiers;
+    py::enum_<Q::ErrorType>(m, "ErrorType")
+        .value("none", Q::ErrorType::none)
+        .value("success", Q::ErrorType::success)
+        .value("invalid_scheme", Q::ErrorType::invalid_scheme)
+        .value("invalid_coeff_modulus_size", Q::ErrorType::invalid_coeff_modulus_size)
+        .value("invalid_coeff_modulus_bit_count", Q::ErrorType::invalid_coeff_modulus_bit_count)
+        .value("invalid_coeff_modulus_no_ntt", Q::ErrorType::invalid_coeff_modulus_no_ntt)
+        .value("invalid_poly_modulus_degree", Q::ErrorType::invalid_poly_modulus_degree)
+        .value("invalid_poly_modulus_degree_non_power_of_two", Q::ErrorType::invalid_poly_modulus_degree_non_power_of_two)
+        .value("invalid_parameters_too_large", Q::ErrorType::invalid_parameters_too_large)
+        .value("invalid_parameters_insecure", Q::ErrorType::invalid_parameters_insecure)
+        .value("failed_creating_rns_base", Q::ErrorType::failed_creating_rns_base)
+        .value("invalid_plain_modulus_bit_count", Q::ErrorType::invalid_plain_modulus_bit_count)
+        .value("invalid_plain_modulus_coprimality", Q::ErrorType::invalid_plain_modulus_coprimality)
+        .value("invalid_plain_modulus_too_large", Q::ErrorType::invalid_plain_modulus_too_large)
+        .value("invalid_plain_modulus_nonzero", Q::ErrorType::invalid_plain_modulus_nonzero)
+        .value("failed_creating_rns_tool", Q::ErrorType::failed_creating_rns_tool);
+    py::class_<Q>(m, "EncryptionParameterQualifiers")
+        .def_readonly("parameter_error", &Q::parameter_error)
+        .def_readonly("using_fft", &Q::using_fft)
+        .def_readonly("using_ntt", &Q::using_ntt)
+        .def_readonly("using_batching", &Q::using_batching)
+        .def_readonly("using_fast_plain_lift", &Q::using_fast_plain_lift)
+        .def_readonly("using_descending_modulus_chain", &Q::using_descending_modulus_chain)
+        .def_readonly("sec_level", &Q::sec_level)
+        .def("parameters_set", &Q::parametersSet)
+        .def("parameter_error_name", &Q::parameterErrorName)
+        .def("parameter_error_message", &Q::parameterErrorMessage);
+    auto words = [](const std::uint64_t *p, std::size_t k) {
+        return p ? to_array(vector<std::uint64_t>(p, p + k)) : py::array_t<std::uint64_t>(0);
+    };
     py::class_<CD, std::shared_ptr<CD>>(m, "ContextData")
         .def("parms", &CD::parms)
         .def("parms_id", &CD::parmsID)
         .def("chain_index", &CD::chainIndex)
+        .def("qualifiers", &CD::qualifiers)
+        .def("total_coeff_modulus_bit_count", &CD::totalCoeffModulusBitCount)
+        .def("total_coeff_modulus",
+             [words](const CD &d) { return words(d.qualifiers().parametersSet() ? d.totalCoeffModulus() : nullptr, d.levelLimbs()); })
+        .def("coeff_div_plain_modulus",
+             [](const CD &d) {
+                 py::list out;
+                 const auto *p = d.coeffDivPlainModulus();
+                 if (p && d.parms().scheme() != SchemeType::ckks && d.qualifiers().parametersSet())
+                     for (int i = 0; i < d.levelLimbs(); i++) out.append(py::make_tuple(p[i].operand, p[i].quotient));
+                 return out;
+             })
+        .def("upper_half_increment",
+             [words](const CD &d) {
+                 const bool ok = d.parms().scheme() != SchemeType::ckks && d.qualifiers().parametersSet();
+                 return words(ok ? d.upperHalfIncrement() : nullptr, d.levelLimbs());
+             })
+        .def("coeff_modulus_mod_plain_modulus", &CD::coeffModulusModPlainModulus)
+        .def("plain_upper_half_threshold", &CD::plainUpperHalfThreshold)
+        .def("plain_upper_half_increment",
+             [words](const CD &d) { return words(d.qualifiers().parametersSet() ? d.plainUpperHalfIncrement() : nullptr, d.levelLimbs()); })
+        .def("upper_half_threshold", [words](const CD &d) { return words(d.upperHalfThreshold(), d.levelLimbs()); })
         .def("prev_context_data", [cd](const CD &d) { return cd(d.prevContextData()); })
         .def("next_context_data", [cd](const CD &d) { return cd(d.nextContextData()); });
 

@@ -278,6 +278,60 @@ static std::string validate(const EncryptionParameters &p, SecurityLevel sec, in
     return "success";
 }
 
+namespace {
+
+using ErrorType = EncryptionParameterQualifiers::ErrorType;
+
+struct ErrorInfo {
+    ErrorType type;
+    const char *name, *message;
+};
+
+// The reference's error names (EncryptionParameterQualifiers::parameterErrorName,
+// src/context.cpp:24-79) with a description of each.
+const ErrorInfo kErrors[] = {
+    {ErrorType::none, "none", "the parameters have not been validated"},
+    {ErrorType::success, "success", "the parameters are valid"},
+    {ErrorType::invalid_scheme, "invalid_scheme", "the scheme is not BFV, CKKS or BGV"},
+    {ErrorType::invalid_coeff_modulus_size, "invalid_coeff_modulus_size", "the number of coefficient moduli is out of range"},
+    {ErrorType::invalid_coeff_modulus_bit_count, "invalid_coeff_modulus_bit_count",
+     "a coefficient modulus has a bit count out of range"},
+    {ErrorType::invalid_coeff_modulus_no_ntt, "invalid_coeff_modulus_no_ntt",
+     "a coefficient modulus is not a prime congruent to 1 modulo 2 * poly_modulus_degree"},
+    {ErrorType::invalid_poly_modulus_degree, "invalid_poly_modulus_degree", "poly_modulus_degree is out of range"},
+    {ErrorType::invalid_poly_modulus_degree_non_power_of_two, "invalid_poly_modulus_degree_non_power_of_two",
+     "poly_modulus_degree is not a power of two"},
+    {ErrorType::invalid_parameters_too_large, "invalid_parameters_too_large", "the parameters are too large"},
+    {ErrorType::invalid_parameters_insecure, "invalid_parameters_insecure",
+     "the coefficient modulus is too large for the security level"},
+    {ErrorType::failed_creating_rns_base, "failed_creating_rns_base", "the coefficient moduli are not pairwise coprime"},
+    {ErrorType::invalid_plain_modulus_bit_count, "invalid_plain_modulus_bit_count",
+     "the plain modulus has a bit count out of range"},
+    {ErrorType::invalid_plain_modulus_coprimality, "invalid_plain_modulus_coprimality",
+     "the plain modulus is not coprime to the coefficient moduli"},
+    {ErrorType::invalid_plain_modulus_too_large, "invalid_plain_modulus_too_large",
+     "the plain modulus is not smaller than the coefficient modulus"},
+    {ErrorType::invalid_plain_modulus_nonzero, "invalid_plain_modulus_nonzero", "CKKS needs a plain modulus of zero"},
+    {ErrorType::failed_creating_rns_tool, "failed_creating_rns_tool", "the RNS tool could not be created"},
+};
+
+const ErrorInfo &error_info(ErrorType t) {
+    for (const auto &e : kErrors)
+        if (e.type == t) return e;
+    return kErrors[0];
+}
+
+ErrorType error_of(const std::string &name) {
+    for (const auto &e : kErrors)
+        if (name == e.name) return e.type;
+    return ErrorType::none;
+}
+
+}  // namespace
+
+const char *EncryptionParameterQualifiers::parameterErrorName() const { return error_info(parameter_error).name; }
+const char *EncryptionParameterQualifiers::parameterErrorMessage() const { return error_info(parameter_error).message; }
+
 // SEALContext::SEALContext (src/context.cpp:458-523): key level, first level (key
 // level minus the special prime), then the chain down while levels stay valid.
 SEALContext::SEALContext(EncryptionParameters parms, bool expand_mod_chain, SecurityLevel sec_level) {
@@ -285,11 +339,68 @@ SEALContext::SEALContext(EncryptionParameters parms, bool expand_mod_chain, Secu
     scheme_ = parms.scheme();
     n_ = parms.polyModulusDegree();
     key_parms_ = parms;
+    // validation and the per-level constants (SEALContext::validate, src/context.cpp:138-425)
     auto make = [&](const EncryptionParameters &p, std::string &err) {
         auto d = std::make_shared<ContextData>();
         d->parms_ = p;
         d->id_ = p.parmsID();
-        err = validate(p, sec_level, d->total_bits_, d->using_batching_);
+        bool batching = false;
+        err = validate(p, sec_level, d->total_bits_, batching);
+        auto &q = d->q_;
+        q.parameter_error = error_of(err);
+        const ErrorType e = q.parameter_error;
+        const bool shape_ok = e != ErrorType::invalid_scheme && e != ErrorType::invalid_coeff_modulus_size &&
+                              e != ErrorType::invalid_coeff_modulus_bit_count &&
+                              e != ErrorType::invalid_poly_modulus_degree &&
+                              e != ErrorType::invalid_poly_modulus_degree_non_power_of_two;
+        q.using_fft = shape_ok;
+        if (shape_ok)
+            q.sec_level = d->total_bits_ > CoeffModulus::MaxBitCount(p.polyModulusDegree(), sec_level) ? SecurityLevel::none
+                                                                                                     : sec_level;
+        q.using_ntt = shape_ok && e != ErrorType::invalid_parameters_insecure &&
+                      e != ErrorType::failed_creating_rns_base && e != ErrorType::invalid_coeff_modulus_no_ntt;
+        q.using_batching = batching;
+        if (e != ErrorType::success) return d;
+        std::vector<uint64_t> qv;
+        for (auto &m : p.coeffModulus()) qv.push_back(m.value());
+        const std::size_t L = qv.size();
+        d->total_ = tb::host::product(qv.data(), L);
+        d->total_.resize(L, 0);
+        q.using_descending_modulus_chain = true;
+        for (std::size_t i = 0; i + 1 < L; i++) q.using_descending_modulus_chain &= qv[i] > qv[i + 1];
+        if (p.scheme() == SchemeType::ckks) {
+            d->plain_thr_ = uint64_t(1) << 63;
+            for (uint64_t qi : qv) d->plain_inc_.push_back(tb::host::mulmod((uint64_t(1) << 63) % qi, qi - 2, qi));
+            d->upper_thr_ = d->total_;   // (Q + 1) / 2
+            for (std::size_t i = 0; i < L && ++d->upper_thr_[i] == 0; i++) {
+            }
+            for (std::size_t i = 0; i < L; i++)
+                d->upper_thr_[i] = (d->upper_thr_[i] >> 1) | (i + 1 < L ? d->upper_thr_[i + 1] << 63 : 0);
+            return d;
+        }
+        const uint64_t t = p.plainModulus().value();
+        q.using_fast_plain_lift = true;
+        for (uint64_t qi : qv) q.using_fast_plain_lift &= qi > t;
+        uint64_t rem = 0;
+        const auto delta = tb::host::div_words(d->total_, t, rem);
+        d->q_mod_t_ = rem;
+        for (uint64_t qi : qv) {
+            const uint64_t v = tb::host::mod_words(delta, qi);
+            d->delta_.push_back({v, tb::host::shoup(v, qi)});
+            d->upper_inc_.push_back(rem % qi);
+        }
+        d->plain_thr_ = (t + 1) >> 1;
+        if (q.using_fast_plain_lift) {
+            for (uint64_t qi : qv) d->plain_inc_.push_back(qi - t);
+        } else {   // Q - t as words
+            d->plain_inc_ = d->total_;
+            uint64_t borrow = t;
+            for (std::size_t i = 0; i < L && borrow; i++) {
+                const uint64_t w = d->plain_inc_[i];
+                d->plain_inc_[i] = w - borrow;
+                borrow = w < borrow ? 1 : 0;
+            }
+        }
         return d;
     };
     auto next_of = [](const EncryptionParameters &p) {

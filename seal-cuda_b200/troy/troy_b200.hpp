@@ -134,8 +134,46 @@ private:
     std::shared_ptr<UniformRandomGeneratorFactory> rng_;
 };
 
+// A constant with its Shoup quotient floor(operand 2^64 / q) (util::MultiplyUIntModOperand,
+// src/utils/uintarithsmallmod.h:166-184).
+struct MultiplyUIntModOperand {
+    std::uint64_t operand = 0, quotient = 0;
+};
+
+// EncryptionParameterQualifiers (src/context.h:20-140): the validation outcome and
+// properties of one level's parameters.
+struct EncryptionParameterQualifiers {
+    enum class ErrorType : int {
+        none = -1,
+        success = 0,
+        invalid_scheme = 1,
+        invalid_coeff_modulus_size = 2,
+        invalid_coeff_modulus_bit_count = 3,
+        invalid_coeff_modulus_no_ntt = 4,
+        invalid_poly_modulus_degree = 5,
+        invalid_poly_modulus_degree_non_power_of_two = 6,
+        invalid_parameters_too_large = 7,
+        invalid_parameters_insecure = 8,
+        failed_creating_rns_base = 9,
+        invalid_plain_modulus_bit_count = 10,
+        invalid_plain_modulus_coprimality = 11,
+        invalid_plain_modulus_too_large = 12,
+        invalid_plain_modulus_nonzero = 13,
+        failed_creating_rns_tool = 14
+    };
+    ErrorType parameter_error = ErrorType::none;
+    bool using_fft = false, using_ntt = false, using_batching = false, using_fast_plain_lift = false,
+         using_descending_modulus_chain = false;
+    SecurityLevel sec_level = SecurityLevel::none;
+    bool parametersSet() const { return parameter_error == ErrorType::success; }
+    const char *parameterErrorName() const;
+    const char *parameterErrorMessage() const;
+};
+
 class SEALContext {
 public:
+    // One level of the modulus chain with the host-side constants of
+    // SEALContext::ContextData (src/context.h:270-460, src/context.cpp:138-425).
     class ContextData {
     public:
         const EncryptionParameters &parms() const { return parms_; }
@@ -145,13 +183,29 @@ public:
         std::shared_ptr<const ContextData> nextContextData() const { return next_; }
         int levelLimbs() const { return (int)parms_.coeffModulus().size(); }
         int totalCoeffModulusBitCount() const { return total_bits_; }
-        bool usingBatching() const { return using_batching_; }
+        bool usingBatching() const { return q_.using_batching; }
+        EncryptionParameterQualifiers qualifiers() const { return q_; }
+        // Q = prod q_i as levelLimbs() little-endian words
+        const std::uint64_t *totalCoeffModulus() const { return total_.data(); }
+        // BFV/BGV: floor(Q / t) mod q_i (Shoup pairs) and (Q mod t) mod q_i
+        const MultiplyUIntModOperand *coeffDivPlainModulus() const { return delta_.data(); }
+        const std::uint64_t *upperHalfIncrement() const { return upper_inc_.data(); }
+        std::uint64_t coeffModulusModPlainModulus() const { return q_mod_t_; }
+        // (t + 1) / 2 (BFV/BGV) or 2^63 (CKKS), and the matching per-limb (q_i - t, or
+        // Q - t as words when some q_i <= t; CKKS: 2^63 (q_i - 2) mod q_i) increments
+        std::uint64_t plainUpperHalfThreshold() const { return plain_thr_; }
+        const std::uint64_t *plainUpperHalfIncrement() const { return plain_inc_.data(); }
+        // CKKS: (Q + 1) / 2 as words
+        const std::uint64_t *upperHalfThreshold() const { return upper_thr_.empty() ? nullptr : upper_thr_.data(); }
 
     private:
         friend class SEALContext;
         EncryptionParameters parms_;
         int total_bits_ = 0;
-        bool using_batching_ = false;
+        EncryptionParameterQualifiers q_;
+        std::vector<std::uint64_t> total_, upper_inc_, plain_inc_, upper_thr_;
+        std::vector<MultiplyUIntModOperand> delta_;
+        std::uint64_t q_mod_t_ = 0, plain_thr_ = 0;
         ParmsID id_{};
         std::size_t chain_index_ = 0;
         std::weak_ptr<const ContextData> prev_;

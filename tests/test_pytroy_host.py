@@ -80,3 +80,56 @@ def test_bfv_default_primes_match_the_reference():
         pytroy.CoeffModulus.bfv_default(4096, L.none)
     with pytest.raises(ValueError):
         pytroy.CoeffModulus.bfv_default(3000)
+
+
+# valid parameters create the device context, so those cases run on the GPU
+_G = pytest.mark.gpu
+
+
+@pytest.mark.skipif(not available("ref"), reason="reference library not built")
+@pytest.mark.parametrize("scheme,n,bits,t,sec", [
+    pytest.param(pytroy.SchemeType.bfv, 4096, [36, 36, 37], 65537, 128, marks=_G),
+    pytest.param(pytroy.SchemeType.bfv, 8192, [43, 43, 44, 44, 44], "batch20", 128, marks=_G),
+    pytest.param(pytroy.SchemeType.bgv, 4096, [30, 30, 30], "prime40", 128, marks=_G),   # t above every q_i
+    pytest.param(pytroy.SchemeType.ckks, 16384, [60] + [40] * 7 + [60], 0, 128, marks=_G),
+    pytest.param(pytroy.SchemeType.bfv, 4096, [60, 60], 65537, 0, marks=_G),              # security none
+    (pytroy.SchemeType.ckks, 4096, [60, 60], 0, 128),                                     # insecure
+    pytest.param(pytroy.SchemeType.bfv, 4096, [36, 36, 37], 1 << 20, 128, marks=_G),       # no batching
+    pytest.param(pytroy.SchemeType.bgv, 4096, [36, 36, 37], 3 * 8191, 128, marks=_G),      # no batching
+    (pytroy.SchemeType.bfv, 4096, [36, 36, 37], "q0", 128),                               # t shares a prime
+])
+def test_context_qualifiers_and_constants_match_the_reference(scheme, n, bits, t, sec):
+    q = [m.value() for m in pytroy.CoeffModulus.create(n, bits)]
+    if t == "batch20":
+        t = pytroy.PlainModulus.batching(n, 20).value()
+    elif t == "prime40":
+        t = pytroy.CoeffModulus.create(n, [40])[0].value()
+    elif t == "q0":
+        t = q[0]
+    ref = Oracle("ref").context_consts(int(scheme.value), n, q, t, sec)
+    p = pytroy.EncryptionParameters(scheme)
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus([pytroy.Modulus(x) for x in q])
+    if scheme != pytroy.SchemeType.ckks:
+        p.set_plain_modulus(t)
+    levels = {0: pytroy.SecurityLevel.none, 128: pytroy.SecurityLevel.tc128}
+    ctx = pytroy.SEALContext(p, True, levels[sec])
+    d = ctx.first_context_data()
+    qual = d.qualifiers()
+    assert int(qual.parameter_error.value) == ref["error"], qual.parameter_error_name()
+    for f in ("using_fft", "using_ntt", "using_batching", "using_fast_plain_lift", "using_descending_modulus_chain"):
+        assert int(getattr(qual, f)) == ref[f], f
+    assert int(qual.sec_level.value) == ref["sec_level"]
+    if not qual.parameters_set():
+        return
+    L = len(d.parms().coeff_modulus())
+    assert list(d.total_coeff_modulus()) == ref["total"][:L]
+    assert d.plain_upper_half_threshold() == ref["plain_upper_half_threshold"]
+    assert list(d.plain_upper_half_increment()) == ref["plain_upper_half_increment"][:L]
+    if scheme == pytroy.SchemeType.ckks:
+        assert list(d.upper_half_threshold()) == ref["upper_half_threshold"][:L]
+    else:
+        assert d.coeff_modulus_mod_plain_modulus() == ref["q_mod_t"]
+        assert [a for a, _ in d.coeff_div_plain_modulus()] == ref["delta"][:L]
+        assert [b for _, b in d.coeff_div_plain_modulus()] == ref["delta_quotient"][:L]
+        assert list(d.upper_half_increment()) == ref["upper_half_increment"][:L]
