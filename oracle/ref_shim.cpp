@@ -196,6 +196,23 @@ int ref_context_consts(int scheme, size_t n, const uint64_t *moduli, int count, 
     }
 }
 
+// Plaintext(hex_poly) and to_string of the reference (src/plaintext.cpp:91-215): the
+// parsed coefficients (count returned; -1 when the string is rejected) and the
+// string printed back.
+int ref_plain_hex(const char *hex, uint64_t *coeffs, size_t cap, char *out, size_t outcap) {
+    try {
+        Plaintext p{std::string(hex)};
+        if (p.coeffCount() > cap) return -2;
+        for (size_t i = 0; i < p.coeffCount(); i++) coeffs[i] = p[i];
+        const std::string s = p.to_string();
+        if (s.size() + 1 > outcap) return -2;
+        std::memcpy(out, s.c_str(), s.size() + 1);
+        return (int)p.coeffCount();
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_plain_modulus_batching(size_t n, int bits, uint64_t *out) {
     try {
         *out = PlainModulus::Batching(n, bits).value();

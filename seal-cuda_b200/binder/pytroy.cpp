@@ -239,6 +239,12 @@ class ParmsID(list):
 
     py::class_<Plaintext>(m, "Plaintext")
         .def(py::init<>())
+        .def(py::init<const std::string &>())
+        .def("to_string", &Plaintext::to_string)
+        .def("__str__", &Plaintext::to_string)
+        .def("is_zero", &Plaintext::isZero)
+        .def("__getitem__", &Plaintext::operator[])
+        .def("__eq__", &Plaintext::operator==)
         .def("set_zero", &Plaintext::setZero)
         .def("coeff_count", &Plaintext::coeffCount)
         .def("is_ntt_form", &Plaintext::isNttForm)
@@ -259,6 +265,7 @@ class ParmsID(list):
         .def("correction_factor", py::overload_cast<>(&Ciphertext::correctionFactor, py::const_))
         .def("set_correction_factor", [](Ciphertext &self, uint64_t c) { self.correctionFactor() = c; })
         .def("resize", py::overload_cast<std::size_t>(&Ciphertext::resize))
+        .def("is_transparent", &Ciphertext::isTransparent)
         .def("reserve", &Ciphertext::reserve)
         .def("parms_id", py::overload_cast<>(&Ciphertext::parmsID, py::const_))
         .def("set_parms_id", [](Ciphertext &self, const ParmsID &p) { self.parmsID() = p; })

@@ -8,9 +8,11 @@
 #include <cuda_runtime_api.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <sstream>
 
 #include "hash.hpp"
 #include "hostmath.hpp"
@@ -492,6 +494,118 @@ void Ciphertext::resize(const SEALContext &context, const ParmsID &parms_id, std
     size_ = size;
     parms_id_ = parms_id;
     data_.resize(size * limbs_ * n_);
+}
+
+namespace {
+
+// hexadecimal digits at p, and the degree of an "x^<decimal>" after them (0 when
+// absent; -1 when malformed)
+int hex_digits(const std::string &s, std::size_t p) {
+    std::size_t k = p;
+    while (k < s.size() && std::isxdigit((unsigned char)s[k])) k++;
+    return (int)(k - p);
+}
+
+long long term_power(const std::string &s, std::size_t p, std::size_t &len) {
+    len = 0;
+    if (p >= s.size() || s[p] != 'x') return 0;
+    if (p + 1 >= s.size() || s[p + 1] != '^') return -1;
+    std::size_t k = p + 2;
+    long long v = 0;
+    while (k < s.size() && std::isdigit((unsigned char)s[k])) {
+        v = v * 10 + (s[k] - '0');
+        if (v > (1ll << 31)) return -1;
+        k++;
+    }
+    if (k == p + 2) return -1;
+    len = k - p;
+    return v;
+}
+
+}  // namespace
+
+Plaintext &Plaintext::operator=(const std::string &hex) {
+    if (isNttForm()) throw std::logic_error("cannot set an NTT transformed Plaintext");
+    struct Term {
+        long long power;
+        uint64_t value;
+    };
+    std::vector<Term> terms;
+    long long last = 1ll << 31;
+    std::size_t pos = 0;
+    while (pos < hex.size()) {
+        const int digits = hex_digits(hex, pos);
+        if (digits == 0) throw std::invalid_argument("unable to parse hex_poly");
+        std::size_t first = pos;
+        while (first < pos + digits - 1 && hex[first] == '0') first++;   // leading zeros
+        if (pos + digits - first > 16) throw std::invalid_argument("hex_poly has too large coefficients");
+        const uint64_t value = std::stoull(hex.substr(first, pos + digits - first), nullptr, 16);
+        pos += digits;
+        std::size_t len = 0;
+        const long long power = term_power(hex, pos, len);
+        if (power < 0 || power >= last) throw std::invalid_argument("unable to parse hex_poly");
+        pos += len;
+        last = power;
+        terms.push_back({power, value});
+        if (pos < hex.size()) {   // " + " between terms (also accepted at the very end)
+            if (hex.compare(pos, 3, " + ") != 0) throw std::invalid_argument("unable to parse hex_poly");
+            pos += 3;
+        }
+    }
+    bool any = false;
+    for (auto &t : terms) any |= t.value != 0;
+    if (terms.empty() || !any) {
+        setZero();
+        return *this;
+    }
+    std::vector<uint64_t> v((std::size_t)terms.front().power + 1, 0);
+    for (auto &t : terms) v[(std::size_t)t.power] = t.value;
+    fromHost(v);
+    return *this;
+}
+
+std::string Plaintext::to_string() const {
+    if (isNttForm()) throw std::invalid_argument("cannot convert NTT transformed plaintext to string");
+    const auto v = toHost();
+    std::ostringstream out;
+    bool empty = true;
+    for (std::size_t i = count_; i-- > 0;) {
+        if (!v[i]) continue;
+        if (!empty) out << " + ";
+        out << std::uppercase << std::hex << v[i] << std::dec;
+        if (i) out << "x^" << i;
+        empty = false;
+    }
+    return empty ? "0" : out.str();
+}
+
+bool Plaintext::isZero() const {
+    for (uint64_t w : toHost())
+        if (w) return false;
+    return true;
+}
+
+uint64_t Plaintext::operator[](std::size_t i) const {
+    if (i >= count_) throw std::out_of_range("coeff_index must be within [0, coeff_count)");
+    uint64_t v = 0;
+    cuda_check(cudaMemcpy(&v, data_.get() + i, 8, cudaMemcpyDeviceToHost), "copy to host");
+    return v;
+}
+
+bool Plaintext::operator==(const Plaintext &o) const {
+    if (parms_id_ != o.parms_id_ || (isNttForm() && scale_ != o.scale_)) return false;
+    auto a = toHost(), b = o.toHost();
+    a.resize(std::max(a.size(), b.size()), 0);
+    b.resize(a.size(), 0);
+    return a == b;
+}
+
+bool Ciphertext::isTransparent() const {
+    if (!data_.size() || size_ < 2) return true;
+    const auto v = toHost();
+    for (std::size_t i = n_ * limbs_; i < v.size(); i++)
+        if (v[i]) return false;
+    return true;
 }
 
 void Ciphertext::fromHost(const std::vector<uint64_t> &v) {

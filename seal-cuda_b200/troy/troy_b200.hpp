@@ -264,6 +264,24 @@ public:
     // Wire format of PlaintextCuda::save/load (src/plaintext_cuda.cu:7-27).
     void save(std::ostream &stream) const;
     void load(std::istream &stream);
+    // The hexadecimal polynomial form "7FFx^3 + 1x^1 + 3" (Plaintext::to_string and
+    // operator=(string), src/plaintext.h:491-498, src/plaintext.cpp:91-215): terms in
+    // strictly decreasing degree joined by " + ", a term without "x^" being degree 0.
+    explicit Plaintext(const std::string &hex_poly) { *this = hex_poly; }
+    Plaintext &operator=(const std::string &hex_poly);
+    std::string to_string() const;
+    bool isZero() const;
+    std::uint64_t operator[](std::size_t i) const;
+    bool operator==(const Plaintext &o) const;
+    std::size_t capacity() const { return count_; }
+    void reserve(std::size_t) {}
+    void shrinkToFit() {}
+    void release() {
+        data_ = DeviceBuffer();
+        count_ = 0;
+        parms_id_ = {0, 0, 0, 0};
+        scale_ = 1.0;
+    }
 
 private:
     DeviceBuffer data_;
@@ -283,6 +301,13 @@ public:
     void resize(const SEALContext &context, std::size_t size) { resize(context, parms_id_, size); }
     // same degree and limb count, `size` polynomials (CiphertextCuda::resize(size_t),
     // src/ciphertext_cuda.cuh:83-88): the common prefix kept, new polynomials zero
+    // true when empty or every polynomial after c0 is zero (CiphertextCuda::isTransparent)
+    bool isTransparent() const;
+    std::size_t sizeCapacity() const { return size_; }
+    void release() {
+        data_ = DeviceBuffer();
+        size_ = 0;
+    }
     void resize(std::size_t size) {
         if ((size < 2 && size != 0) || size > 16) throw std::invalid_argument("invalid size");
         data_.resize(size * limbs_ * n_);

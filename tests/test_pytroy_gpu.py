@@ -6,6 +6,7 @@ tests/golden/gen_golden.py); the rest of the evaluator surface is checked by
 decryption against plaintext arithmetic, in the style of the reference's own
 evaluator tests (test/evaluator_cuda.cu). Overloads are called as the reference
 module registers them (e.g. the returning mod_switch_to takes the parms_id first)."""
+import json
 import os
 
 import numpy as np
@@ -423,3 +424,21 @@ def test_two_party_flow_like_the_reference_binder_test():
     out.load(x.save())
     got = a_enc.decode(pytroy.Decryptor(a_ctx, keygen.secret_key()).decrypt(out))
     assert np.abs(got[:3] - np.array([1.2, 2.1, 3.2])).max() < 1e-5
+
+
+def test_plaintext_hex_strings_match_the_reference():
+    """Parsing and printing of hexadecimal polynomials against the reference's own
+    results (tests/golden/hex_poly.json, made by tests/golden/gen_hex_poly.py)."""
+    with open(os.path.join(G, "hex_poly.json")) as f:
+        cases = json.load(f)
+    for case in cases:
+        text = case["text"]
+        if not case["accepted"]:
+            with pytest.raises(ValueError):
+                pytroy.Plaintext(text)
+            continue
+        p = pytroy.Plaintext(text)
+        coeffs = [int(c) for c in case["coeffs"]]
+        assert p.to_string() == case["printed"], text
+        assert [p[i] for i in range(p.coeff_count())] == coeffs, text
+        assert p.is_zero() == (not any(coeffs))
