@@ -1,6 +1,8 @@
 // The extern "C" boundary (include/troy_b200.h): argument checks, device selection
 // and status conversion around the internal launchers.
+#include <cstdint>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <string>
 
@@ -97,6 +99,18 @@ int on_device(const tb_context *ctx, F &&f) {
     return st;
 }
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// The transform kernels move coefficient pairs as 16-byte words, so coefficient
+// buffers must start on 16-byte boundaries and strides (in words) must be even; a
+// call that breaks this is refused here rather than faulting on the device.
+int require_vec(std::initializer_list<const void *> ptrs, std::initializer_list<uint64_t> strides) {
+    for (const void *p : ptrs)
+        if (p && (reinterpret_cast<uintptr_t>(p) & 15u))
+            return set_error(tb::TB_ERR_INVALID_ARGUMENT, "device buffers must start on 16-byte boundaries");
+    for (uint64_t st : strides)
+        if (st & 1) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "strides must be even numbers of words");
+    return tb::TB_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -157,21 +171,25 @@ int tb_context_moduli(const tb_context *ctx, uint64_t *out, int capacity, int *c
 
 int tb_ntt_forward(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, int lazy,
                    void *stream) {
+    if (const int vst = require_vec({in, out}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) { return tb::ntt_forward(c, in, out, polys, first, limbs, lazy != 0, S(stream)); });
 }
 
 int tb_ntt_inverse(tb_context *ctx, const uint64_t *in, uint64_t *out, uint64_t polys, int first, int limbs, int lazy,
                    void *stream) {
+    if (const int vst = require_vec({in, out}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) { return tb::ntt_inverse(c, in, out, polys, first, limbs, lazy != 0, S(stream)); });
 }
 
 int tb_dyadic_product(tb_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t polys, int first,
                       int limbs, void *stream) {
+    if (const int vst = require_vec({a, b, out}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) { return tb::dyadic_product(c, a, b, out, polys, first, limbs, S(stream)); });
 }
 
 int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b,
                       uint64_t b_stride, uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({a, b, out}, {a_stride, b_stride, out_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::tensor_product(c, first, L, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
     });
@@ -179,6 +197,7 @@ int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint
 
 int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b, uint64_t b_stride,
                 uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({a, b, out}, {a_stride, b_stride, out_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::multiply(c, L, a, a_stride, b, b_stride, out, out_stride, batch, S(stream));
     });
@@ -186,11 +205,13 @@ int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, co
 
 int tb_multiply_sizes(tb_context *ctx, int L, const uint64_t *a, int a_size, const uint64_t *b, int b_size,
                       uint64_t *out, void *stream) {
+    if (const int vst = require_vec({a, b, out}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) { return tb::multiply_sizes(c, L, a, a_size, b, b_size, out, S(stream)); });
 }
 
 int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target_stride, uint64_t *ct,
                  uint64_t ct_stride, const uint64_t *key, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({target, ct, key}, {target_stride, ct_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::keyswitch(c, L, target, target_stride, ct, ct_stride, key, batch, S(stream));
     });
@@ -198,6 +219,7 @@ int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target
 
 int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key, uint64_t batch,
                    void *stream) {
+    if (const int vst = require_vec({ct, key}, {ct_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         const uint64_t stride = ct_stride ? ct_stride : 3ull * L * c.n;
         if (!ct) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null buffer");
@@ -207,6 +229,7 @@ int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, con
 
 int tb_relinearize_noalloc(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key,
                            uint64_t batch, void *stream) {
+    if (const int vst = require_vec({ct, key}, {ct_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::relinearize_noalloc(c, L, ct, ct_stride, key, batch, S(stream));
     });
@@ -214,6 +237,7 @@ int tb_relinearize_noalloc(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_str
 
 int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t *in, uint64_t in_stride,
                     uint64_t *out, uint64_t out_stride, const uint64_t *key, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({in, out, key}, {in_stride, out_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::apply_galois(c, L, galois_elt, in, in_stride, out, out_stride, key, batch, S(stream));
     });
@@ -222,6 +246,7 @@ int tb_apply_galois(tb_context *ctx, int L, uint32_t galois_elt, const uint64_t 
 int tb_apply_galois_groups(tb_context *ctx, int L, int groups, const uint32_t *elts, const uint64_t *counts,
                            const uint64_t *in, uint64_t in_stride, uint64_t *out, uint64_t out_stride,
                            const uint64_t *const *keys, void *stream) {
+    if (const int vst = require_vec({in, out}, {in_stride, out_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::apply_galois_groups(c, L, groups, elts, counts, in, in_stride, out, out_stride, keys, S(stream));
     });
@@ -234,6 +259,7 @@ int tb_galois_elt_from_step(const tb_context *ctx, int step, uint32_t *elt) {
 
 int tb_rescale_to_next(tb_context *ctx, int L, const uint64_t *in, uint64_t in_stride, uint64_t *out,
                        uint64_t out_stride, int size, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({in, out}, {in_stride, out_stride})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         return tb::rescale_to_next(c, L, in, in_stride, out, out_stride, size, batch, S(stream));
     });
@@ -280,6 +306,7 @@ int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t 
 }
 
 int tb_expand_seeded(tb_context *ctx, int L, uint64_t seed, int inverse_ntt, uint64_t *c1, void *stream) {
+    if (const int vst = require_vec({c1}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) { return tb::expand_seeded(c, L, seed, inverse_ntt != 0, c1, S(stream)); });
 }
 
@@ -343,6 +370,7 @@ int tb_ckks_encode_int64(tb_context *ctx, int L, int64_t value, uint64_t *plain,
 
 int tb_plain_to_ntt(tb_context *ctx, int L, const uint64_t *plain, uint64_t plain_stride, uint64_t plain_count,
                     uint64_t *out, uint64_t batch, void *stream) {
+    if (const int vst = require_vec({out}, {})) return vst;
     return on_device(ctx, [&](tb::Context &c) {
         if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
         return tb::plain_to_ntt(c, L, plain, plain_stride, (uint32_t)plain_count, out, batch, S(stream));

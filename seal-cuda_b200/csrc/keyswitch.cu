@@ -260,14 +260,19 @@ struct ModDownBase {
 struct ModDownCkksOp : ModDownBase {
     __device__ Ctx ctx(int b) const { return make(b); }
     __device__ uint64_t load(const Ctx &c, int e) const { return last_mod(c, e) + c.d.fix; }
-    __device__ uint64_t fin(const Ctx &c, int e, uint64_t v) const {
-        const uint64_t q = c.lm.q;
-        const uint64_t x = c.acc[e] + 4 * q - v;
-        return add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), c.ct[e], q);
+    // epilogue reads of a coefficient pair: the accumulator and the ciphertext limb
+    struct Epi {
+        ulonglong2 acc, ct;
+    };
+    __device__ Epi epi2(const Ctx &c, int e) const {
+        return {*reinterpret_cast<const ulonglong2 *>(c.acc + e), *reinterpret_cast<const ulonglong2 *>(c.ct + e)};
     }
-    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
-        const uint64_t x = fin(c, e, a), y = fin(c, e + 1, b);
-        *reinterpret_cast<ulonglong2 *>(c.ct + e) = make_ulonglong2(x, y);
+    __device__ uint64_t fin(const Ctx &c, uint64_t acc, uint64_t ct, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        return add_mod(mul_shoup(acc + 4 * q - v, c.d.inv, c.d.inv_quo, q), ct, q);
+    }
+    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {
+        *reinterpret_cast<ulonglong2 *>(c.ct + e) = make_ulonglong2(fin(c, p.acc.x, p.ct.x, a), fin(c, p.acc.y, p.ct.y, b));
     }
 };
 

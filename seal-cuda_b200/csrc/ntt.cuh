@@ -21,6 +21,8 @@
 
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace tb {
@@ -138,6 +140,47 @@ __device__ __forceinline__ void fwd_passes(const Op &op, const Ctx &c, uint64_t 
     }
 }
 
+// Copy-out of a forward transform: coefficient pairs (e, e+1) from shared memory to
+// op.store2. An Op whose epilogue reads global memory declares `Epi` with
+// epi2(ctx, e) (the reads for a pair) and store2(ctx, e, a, b, epi): the reads of
+// four pairs are then issued before any of their stores, so the epilogue keeps
+// several loads in flight instead of one pair's at a time.
+template <class Op, class = void>
+struct HasEpi : std::false_type {};
+template <class Op>
+struct HasEpi<Op, std::void_t<typename Op::Epi>> : std::true_type {};
+
+template <int NB, int T, class Op, class Ctx>
+__device__ __forceinline__ void fwd_copy_out(const Op &op, const Ctx &c, const uint64_t *sm, int off) {
+    constexpr int ITER = NB / (2 * T);
+    if constexpr (HasEpi<Op>::value && ITER >= 1 && NB % (2 * T) == 0) {
+        constexpr int BATCH = ITER >= 4 ? 4 : ITER;
+        static_assert(ITER % BATCH == 0, "copy-out batches");
+#pragma unroll
+        for (int i0 = 0; i0 < ITER; i0 += BATCH) {
+            typename Op::Epi pre[BATCH];
+#pragma unroll
+            for (int i = 0; i < BATCH; i++) pre[i] = op.epi2(c, threadIdx.x * 2 + (i0 + i) * 2 * T + off);
+#pragma unroll
+            for (int i = 0; i < BATCH; i++) {
+                const int e = threadIdx.x * 2 + (i0 + i) * 2 * T;
+                const int p = swz(e);
+                const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
+                if (p & 1) op.store2(c, e + off, w.y, w.x, pre[i]);
+                else op.store2(c, e + off, w.x, w.y, pre[i]);
+            }
+        }
+    } else {
+        for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
+            const int p = swz(e);
+            const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
+            const uint64_t a = (p & 1) ? w.y : w.x, b = (p & 1) ? w.x : w.y;
+            if constexpr (HasEpi<Op>::value) op.store2(c, e + off, a, b, op.epi2(c, e + off));
+            else op.store2(c, e + off, a, b);
+        }
+    }
+}
+
 template <int LOGB, int V, class Op>
 __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op, int s0) {
     extern __shared__ uint64_t sm[];
@@ -149,13 +192,7 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op
     constexpr int FIRST = REM != 0 ? REM : 3;
     fwd_pass<FIRST, true, LOGB, T, 0, false>(op, c, sm, rbase);
     fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
-    // coalesced copy-out, two coefficients per thread
-    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
-        const int p = swz(e);
-        const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
-        if (p & 1) op.store2(c, e, w.y, w.x);
-        else op.store2(c, e, w.x, w.y);
-    }
+    fwd_copy_out<NB, T>(op, c, sm, 0);   // coalesced, two coefficients per thread
 }
 
 // ---------------------------------------------------------------- inverse
@@ -301,12 +338,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THR
     constexpr int FIRST = REM != 0 ? REM : 3;
     fwd_pass<FIRST, false, LOGB, T, 0, false>(op, c, sm, rbase);
     fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
-    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
-        const int p = swz(e);
-        const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
-        if (p & 1) op.store2(c, e + off, w.y, w.x);
-        else op.store2(c, e + off, w.x, w.y);
-    }
+    fwd_copy_out<NB, T>(op, c, sm, off);
 }
 
 template <int LOGB, class Op>

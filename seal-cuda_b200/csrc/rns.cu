@@ -130,12 +130,17 @@ struct RescaleNttOp {
         }
         return x + c.d.fix;
     }
-    __device__ uint64_t fin(const Ctx &c, int e, uint64_t v) const {
+    // epilogue reads of a coefficient pair: the limb being rescaled
+    struct Epi {
+        ulonglong2 in;
+    };
+    __device__ Epi epi2(const Ctx &c, int e) const { return {*reinterpret_cast<const ulonglong2 *>(c.in + e)}; }
+    __device__ uint64_t fin(const Ctx &c, uint64_t in, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        return mul_shoup(c.in[e] + 4 * q - v, c.d.inv, c.d.inv_quo, q);
+        return mul_shoup(in + 4 * q - v, c.d.inv, c.d.inv_quo, q);
     }
-    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
-        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(fin(c, e, a), fin(c, e + 1, b));
+    __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {
+        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(fin(c, p.in.x, a), fin(c, p.in.y, b));
     }
 };
 

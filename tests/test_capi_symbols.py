@@ -22,3 +22,18 @@ def test_invalid_arguments_fail_loudly_without_touching_the_device():
     assert b"1 mod 2N" in lib.tb_last_error()
     st = lib.tb_context_create(0, ctypes.c_uint64(48), arr, 1, ctypes.c_uint64(0), ctypes.byref(h))
     assert st == 1
+
+
+def test_misaligned_buffers_and_odd_strides_are_refused_on_the_host():
+    """Transform entry points take coefficient pairs as 16-byte words: a buffer off a
+    16-byte boundary or an odd stride is an error status, never a device access."""
+    lib = tb_capi.lib()
+    base = 1 << 20   # a fake, never-dereferenced address
+    v = ctypes.c_void_p
+    st = lib.tb_ntt_forward(None, v(base + 8), v(base), ctypes.c_uint64(1), 0, 1, 0, None)
+    assert st == 1 and b"16-byte" in lib.tb_last_error()
+    st = lib.tb_rescale_to_next(None, 2, v(base), ctypes.c_uint64(3), v(base), ctypes.c_uint64(0), 2,
+                                ctypes.c_uint64(1), None)
+    assert st == 1 and b"even" in lib.tb_last_error()
+    st = lib.tb_relinearize(None, 2, v(base), ctypes.c_uint64(0), v(base + 4), ctypes.c_uint64(1), None)
+    assert st == 1 and b"16-byte" in lib.tb_last_error()
