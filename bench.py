@@ -13,7 +13,9 @@ prime (the arithmetic performed is the same as on encrypted data).
 * ``value``: ops/s with inputs resident in HBM (CUDA events on the launch stream,
   max over ranks). Inputs (2 x 128 MB) exceed the 126 MB L2 between steps.
 * ``e2e``: the same metric through the C ABI with host buffers: every step copies
-  both operand batches from pinned host memory and reads the results back.
+  both operand batches from pinned host memory and reads the results back; the
+  copies run on one stream per direction, overlapping the neighbouring steps'
+  arithmetic (two device buffer sets, ordered by events).
 * ``roofline``: the dominant kernel from the library's per-launch event trace.
 * ``cpu_baseline``: the reference's own CPU implementation (compiled under
   oracle/_ref) on a bounded sample of the same workload, one process per core.
@@ -186,11 +188,11 @@ def run_b200(args, rank, world):
     C = (ctypes.c_uint64 * len(runs))(*[cnt for _, _, cnt in runs])
     P = (ctypes.c_void_p * len(runs))(*[gks[g].data_ptr() for g, _, _ in runs])
 
-    def step(a, b, out):
-        ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, stream)
-        ctx("relinearize", L, T3, 0, rlk, PAIRS, stream)
-        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, stream)
-        ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, stream)
+    def step(a, b, out, st=stream):
+        ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, st)
+        ctx("relinearize", L, T3, 0, rlk, PAIRS, st)
+        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, st)
+        ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, st)
 
     def barrier():
         if world > 1:
@@ -202,7 +204,7 @@ def run_b200(args, rank, world):
     # (NTT launch variants, key-switch budget; all compute identical words) and keeps
     # the fastest
     import tuning
-    tuned = tuning.tune_step(lambda: step(A, B, O), 14, stream)
+    tuned = "off" if args.no_tune else tuning.tune_step(lambda: step(A, B, O), 14, stream)
     for _ in range(args.warmup):
         step(A, B, O)
     barrier()
@@ -247,26 +249,59 @@ def run_b200(args, rank, world):
     barrier()
     per_op_ms = e0.elapsed_time(e1) / per_op_pairs
 
-    # end to end through the C ABI with host buffers
+    # End to end through the C ABI with host buffers: every step copies its inputs in
+    # from page-locked host memory and its results back out. The copies run on their
+    # own streams (one per direction) with two device buffer sets, so step k's inputs
+    # arrive while step k-1 computes and step k-2's results leave; events order each
+    # buffer's reuse.
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
-    hO = torch.empty(O.shape, dtype=torch.int64, pin_memory=True)
+    hO = [torch.empty(O.shape, dtype=torch.int64, pin_memory=True) for _ in range(2)]
     hA.copy_(A)
     hB.copy_(B)
-    dA, dB = torch.empty_like(A), torch.empty_like(B)
+    dA = [torch.empty_like(A) for _ in range(2)]
+    dB = [torch.empty_like(B) for _ in range(2)]
+    dO = [O, torch.empty_like(O)]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event()
+    pending = {}
 
-    def e2e_step():
-        dA.copy_(hA, non_blocking=True)
-        dB.copy_(hB, non_blocking=True)
-        step(dA, dB, O)
-        hO.copy_(O, non_blocking=True)
+    def e2e_step(k):
+        j = k % 2
+        arrived, computed, left = ev(), ev(), ev()
+        with torch.cuda.stream(s_in):
+            if ("computed", k - 2) in pending:
+                s_in.wait_event(pending.pop(("computed", k - 2)))   # step k-2 done reading dA[j], dB[j]
+            dA[j].copy_(hA, non_blocking=True)
+            dB[j].copy_(hB, non_blocking=True)
+            arrived.record(s_in)
+        stream.wait_event(arrived)
+        if ("left", k - 2) in pending:
+            stream.wait_event(pending.pop(("left", k - 2)))          # dO[j] read out
+        step(dA[j], dB[j], dO[j])
+        computed.record(stream)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(computed)
+            hO[j].copy_(dO[j], non_blocking=True)
+            left.record(s_out)
+        pending[("computed", k)] = computed
+        pending[("left", k)] = left
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
+    def e2e_run(first, count):
+        start = ev()
+        start.record(stream)            # the copy streams begin after the timed start
+        s_in.wait_event(start)
+        s_out.wait_event(start)
+        for k in range(first, first + count):
+            e2e_step(k)
+        for key in [key for key in pending if key[0] == "left"]:
+            stream.wait_event(pending[key])                          # every result is on the host
+        pending.clear()
+
+    e2e_run(0, max(1, args.warmup))
     barrier()
     e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
+    e2e_run(0, args.steps)
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -681,6 +716,8 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
     ap.add_argument("--no-ntt-sweep", action="store_true", help="skip the raw transform sweep")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference CUDA path")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch settings (for profiler captures: no tuning launches first)")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
                     help="ciphertext pairs per step (smaller cases for profiling)")
     args = ap.parse_args()
