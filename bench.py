@@ -603,9 +603,10 @@ def roofline(res, steps):
 
 
 # DRAM bytes (read + write) per step of a kernel, from an ncu capture of a smaller
-# batch of this workload scaled by the units processed (see profiles/); absent until
-# captured.
-TRAFFIC_PER_STEP: dict = {}
+# batch of this workload scaled by the units processed: the mod-up launch at L = 8 of
+# 16 ciphertexts moved 19.268608 + 75.146240 MB; a step runs it for 64 ciphertexts at
+# L = 8 (x4) and at L = 7 (x4 x (7 + 49) / (8 + 64) target limbs and digits).
+TRAFFIC_PER_STEP: dict = {"ks_modup_ntt": (19.268608e6 + 75.146240e6) * 4 * (1 + 56 / 72)}
 
 
 # -------------------------------------------------------------- CPU baseline
