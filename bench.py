@@ -82,15 +82,19 @@ def _peak_hbm():
 # ------------------------------------------------------------ clocks sampler
 class ClockSampler:
     """Samples the SM clock and the clock-event (throttle) reasons of the benchmark's
-    GPU every 5 ms through NVML while the timed region runs, so that even a region
-    of a few tens of milliseconds gets samples; falls back to nvidia-smi."""
+    GPU every 2 ms through NVML. start() returns once sampling runs; only the samples
+    taken between mark() (the timed region's start) and stop() are reported, so even a
+    region of a few tens of milliseconds gets several samples."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+    PERIOD_S = 0.002
 
     def __init__(self, device):
         self.device = device
-        self.samples, self.mask, self.max_mhz = [], 0, None
+        self.samples, self.max_mhz = [], None
+        self.begin = 0
         self.stop_flag = threading.Event()
+        self.ready = threading.Event()
         self.t = None
         self.err = None
 
@@ -113,26 +117,35 @@ class ClockSampler:
             reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
                 pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
             while not self.stop_flag.is_set():
-                self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
-                self.mask |= int(reasons(h))
-                time.sleep(0.005)
+                self.samples.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), int(reasons(h))))
+                self.ready.set()
+                time.sleep(self.PERIOD_S)
         except Exception as e:  # NVML missing or refused: report it
             self.err = f"{type(e).__name__}: {e}"
+        finally:
+            self.ready.set()
 
     def start(self):
         self.t = threading.Thread(target=self._run, daemon=True)
         self.t.start()
-        time.sleep(0.02)
+        self.ready.wait(timeout=10)
+
+    def mark(self):
+        self.begin = len(self.samples)
 
     def stop(self):
         self.stop_flag.set()
         if self.t:
             self.t.join(timeout=5)
-        if self.err or not self.samples:
+        taken = self.samples[self.begin:] or self.samples[-1:]
+        if self.err or not taken:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [self.err or "no samples"], "samples": 0}
-        reasons = sorted(k for k, bit in self.REASONS.items() if self.mask & bit)
-        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                "samples": len(self.samples), "source": "NVML every 5 ms"}
+        mask = 0
+        for _, m in taken:
+            mask |= m
+        reasons = sorted(k for k, bit in self.REASONS.items() if mask & bit)
+        return {"sm_mhz": statistics.median(mhz for mhz, _ in taken), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(taken), "source": "NVML every 2 ms during the timed region"}
 
 
 def _rand_residues(torch, shape, moduli, gen):
@@ -213,6 +226,7 @@ def run_b200(args, rank, world):
     lib.tb_trace_enable(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")
+    clocks.mark()
     e0.record(stream)
     for _ in range(args.steps):
         step(A, B, O)
