@@ -161,13 +161,23 @@ __device__ __forceinline__ uint64_t pw(const uint64_t *K, int off, int i, uint64
     return mul_shoup(x, K[off + 2 * i], K[off + 2 * i + 1], q);
 }
 
+// The per-coefficient BEHZ kernels are templates over the data-limb count LT, with LT = 0
+// the run-time form for any count up to MAXL. With LT fixed the loops over the data limbs
+// unroll and the per-coefficient residues and accumulators stay in registers; the loops
+// over the B / Bsk primes stay rolled, so one iteration's constants are all that is live
+// beside them.
+
 // Steps (1)+(2): q (coefficient form) -> Bsk, one coefficient per thread, for both
 // inputs of B products: polynomial p = ct*4 + slot, slots 0,1 from a and 2,3 from b;
 // output [B][4][bsk][N].
-__global__ void behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astride, const uint64_t *__restrict__ b,
-                                 uint64_t bstride, uint64_t *__restrict__ dst, const Mod *__restrict__ qm,
-                                 const Mod *__restrict__ bm, const uint64_t *__restrict__ K, RnsOff o, int L,
-                                 int bsk, int logn, uint64_t P) {
+template <int LT>
+__global__ void __launch_bounds__(256) behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astride,
+                                                        const uint64_t *__restrict__ b, uint64_t bstride,
+                                                        uint64_t *__restrict__ dst, const Mod *__restrict__ qm,
+                                                        const Mod *__restrict__ bm, const uint64_t *__restrict__ K,
+                                                        RnsOff o, int L_, int bsk, int logn, uint64_t P) {
+    constexpr int NL = LT > 0 ? LT : MAXL, UNROLL = LT > 0 ? LT : 1;
+    const int L = LT > 0 ? LT : L_;
     const uint32_t n = 1u << logn;
     const uint64_t total = P << logn;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
@@ -176,18 +186,25 @@ __global__ void behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astrid
         const uint64_t ct = p >> 2, slot = p & 3;
         const uint64_t *in = (slot < 2 ? a + ct * astride + ((slot * L) << logn)
                                        : b + ct * bstride + (((slot - 2) * L) << logn)) + e;
-        uint64_t tmp[MAXL];
+        uint64_t tmp[NL];
         uint64_t mt = 0;
-        for (int i = 0; i < L; i++) {
+#pragma unroll UNROLL
+        for (int i = 0; i < NL; i++) {
+            if (i >= L) break;
             tmp[i] = pw(K, o.q_mtip, i, in[(size_t)i << logn], qm[i].value);
             mt += tmp[i] * K[o.M_qB + bsk * L + i];
         }
         const uint64_t r = ((mt & 0xffffffffull) * K[o.neg_inv_q_mt]) & 0xffffffffull;
         uint64_t *out = dst + ((p * bsk) << logn) + e;
+#pragma unroll 1
         for (int k = 0; k < bsk; k++) {
-            const Mod m = bm[k];
+            const Mod &m = bm[k];
             U128 acc{0, 0};
-            for (int i = 0; i < L; i++) mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
+#pragma unroll UNROLL
+            for (int i = 0; i < NL; i++) {
+                if (i >= L) break;
+                mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
+            }
             const uint64_t v = reduce128(acc.hi, acc.lo, m);
             const uint64_t rr = r >= (1ull << 31) ? r + m.value - (1ull << 32) : r;
             const uint64_t y = add_mod(pw(K, o.Qmod_b, k, rr, m.value), v, m.value);
@@ -196,11 +213,18 @@ __global__ void behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astrid
     }
 }
 
-// Steps (6)-(8): (q U Bsk, inverse-NTT outputs) -> q, one coefficient per thread.
-__global__ void behz_floor_sk_kernel(const uint64_t *__restrict__ tq, const uint64_t *__restrict__ tbk,
-                                     uint64_t *__restrict__ out, uint64_t ostride, const Mod *__restrict__ qm,
-                                     const Mod *__restrict__ bm, const uint64_t *__restrict__ K, RnsOff o, int L,
-                                     int bB, int logn, uint64_t P) {
+// Steps (6)-(8): (q U Bsk, inverse-NTT outputs) -> q, one coefficient per thread. The
+// floor residue of each B prime feeds the Shenoy-Kumaresan sums (into every q_i and into
+// m_sk) as soon as it is made, so no per-prime array is kept.
+template <int LT>
+__global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *__restrict__ tq,
+                                                            const uint64_t *__restrict__ tbk,
+                                                            uint64_t *__restrict__ out, uint64_t ostride,
+                                                            const Mod *__restrict__ qm, const Mod *__restrict__ bm,
+                                                            const uint64_t *__restrict__ K, RnsOff o, int L_, int bB,
+                                                            int logn, uint64_t P) {
+    constexpr int NL = LT > 0 ? LT : MAXL, UNROLL = LT > 0 ? LT : 1;
+    const int L = LT > 0 ? LT : L_;
     const int bsk = bB + 1;
     const uint32_t n = 1u << logn;
     const uint64_t total = P << logn;
@@ -209,39 +233,92 @@ __global__ void behz_floor_sk_kernel(const uint64_t *__restrict__ tq, const uint
         const uint32_t e = (uint32_t)(w & (n - 1));
         const uint64_t *iq = tq + ((p * L) << logn) + e;
         const uint64_t *ib = tbk + ((p * bsk) << logn) + e;
-        uint64_t tmp[MAXL];
-        for (int i = 0; i < L; i++) {
+        uint64_t tmp[NL];
+#pragma unroll UNROLL
+        for (int i = 0; i < NL; i++) {
+            if (i >= L) break;
             const uint64_t q = qm[i].value;
             tmp[i] = pw(K, o.q_ip, i, pw(K, o.t_q, i, iq[(size_t)i << logn], q), q);
         }
-        uint64_t fl[MAXB];
-        for (int k = 0; k < bsk; k++) {
-            const Mod m = bm[k];
+        // floor residue of Bsk prime k: (t * ct_k - conv_k(t * ct_q)) / q mod m_k
+        auto floor_residue = [&](int k) {
+            const Mod &m = bm[k];
             U128 acc{0, 0};
-            for (int i = 0; i < L; i++) mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
+#pragma unroll UNROLL
+            for (int i = 0; i < NL; i++) {
+                if (i >= L) break;
+                mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
+            }
             const uint64_t conv = reduce128(acc.hi, acc.lo, m);
             const uint64_t bv = pw(K, o.t_b, k, ib[(size_t)k << logn], m.value);
-            fl[k] = pw(K, o.inv_q_b, k, bv + m.value - conv, m.value);
-        }
+            return pw(K, o.inv_q_b, k, bv + m.value - conv, m.value);
+        };
         // Shenoy-Kumaresan: B -> q with the m_sk correction
-        for (int k = 0; k < bB; k++) fl[k] = pw(K, o.B_ip, k, fl[k], bm[k].value);
-        const Mod ms = bm[bB];
-        U128 acc{0, 0};
-        for (int k = 0; k < bB; k++) mac128(acc, fl[k], K[o.M_Bmsk + k]);
-        const uint64_t tmsk = reduce128(acc.hi, acc.lo, ms);
-        const uint64_t alpha = mul_shoup(tmsk + (ms.value - fl[bB]), K[o.inv_pb_msk], K[o.inv_pb_msk + 1], ms.value);
+        U128 acc_q[NL];
+#pragma unroll UNROLL
+        for (int i = 0; i < NL; i++) acc_q[i] = U128{0, 0};
+        U128 acc_sk{0, 0};
+#pragma unroll 1
+        for (int k = 0; k < bB; k++) {
+            const uint64_t f = pw(K, o.B_ip, k, floor_residue(k), bm[k].value);
+            mac128(acc_sk, f, K[o.M_Bmsk + k]);
+#pragma unroll UNROLL
+            for (int i = 0; i < NL; i++) {
+                if (i >= L) break;
+                mac128(acc_q[i], f, K[o.M_Bq + i * bB + k]);
+            }
+        }
+        const Mod &ms = bm[bB];
+        const uint64_t fsk = floor_residue(bB);
+        const uint64_t tmsk = reduce128(acc_sk.hi, acc_sk.lo, ms);
+        const uint64_t alpha = mul_shoup(tmsk + (ms.value - fsk), K[o.inv_pb_msk], K[o.inv_pb_msk + 1], ms.value);
         const bool neg = alpha > (ms.value >> 1);
         uint64_t *dst = out + (p / 3) * ostride + (((p % 3) * L) << logn) + e;
-        for (int i = 0; i < L; i++) {
-            const Mod m = qm[i];
-            U128 a{0, 0};
-            for (int k = 0; k < bB; k++) mac128(a, fl[k], K[o.M_Bq + i * bB + k]);
-            const uint64_t d = reduce128(a.hi, a.lo, m);
+#pragma unroll UNROLL
+        for (int i = 0; i < NL; i++) {
+            if (i >= L) break;
+            const Mod &m = qm[i];
+            const uint64_t d = reduce128(acc_q[i].hi, acc_q[i].lo, m);
             const uint64_t corr = neg ? pw(K, o.pb_q, i, ms.value - alpha, m.value) : pw(K, o.negpb_q, i, alpha, m.value);
             dst[(size_t)i << logn] = add_mod(corr, d, m.value);
         }
     }
 }
+
+template <int LT>
+struct LiftLaunch {
+    template <class... A>
+    static cudaError_t run(uint64_t threads, cudaStream_t s, A... args) {
+        behz_lift_kernel<LT><<<grid_for(threads, 256), 256, 0, s>>>(args...);
+        return cudaGetLastError();
+    }
+};
+
+template <int LT>
+struct FloorLaunch {
+    template <class... A>
+    static cudaError_t run(uint64_t threads, cudaStream_t s, A... args) {
+        behz_floor_sk_kernel<LT><<<grid_for(threads, 256), 256, 0, s>>>(args...);
+        return cudaGetLastError();
+    }
+};
+
+// Launches a BEHZ kernel with the data-limb count fixed for L <= 16, the run-time form
+// otherwise.
+#define TB_BEHZ_CASE(LV) \
+    case LV:             \
+        return Launch<LV>::run(threads, s, args...);
+template <template <int> class Launch, class... A>
+cudaError_t behz_dispatch(int L, uint64_t threads, cudaStream_t s, A... args) {
+    switch (L) {
+        TB_BEHZ_CASE(1) TB_BEHZ_CASE(2) TB_BEHZ_CASE(3) TB_BEHZ_CASE(4) TB_BEHZ_CASE(5) TB_BEHZ_CASE(6)
+        TB_BEHZ_CASE(7) TB_BEHZ_CASE(8) TB_BEHZ_CASE(9) TB_BEHZ_CASE(10) TB_BEHZ_CASE(11) TB_BEHZ_CASE(12)
+        TB_BEHZ_CASE(13) TB_BEHZ_CASE(14) TB_BEHZ_CASE(15) TB_BEHZ_CASE(16)
+    default:
+        return Launch<0>::run(threads, s, args...);
+    }
+}
+#undef TB_BEHZ_CASE
 
 // NTT over a packed [P][limbs][N] buffer; limb l uses mods[l] (chain or Bsk array).
 template <bool FWD>
@@ -402,9 +479,9 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     }
     {
         TraceScope ts("bfv_lift", s);
-        behz_lift_kernel<<<grid_for(4 * B * n, 256), 256, 0, s>>>(a, astride, b, bstride, xb, c.d_mods, lv.d_bsk_mods,
-                                                                 lv.d_consts, lv.off, L, bsk, logn, 4 * B);
-        e = cudaGetLastError();
+        e = behz_dispatch<LiftLaunch>(L, 4 * B * n, s, a, astride, b, bstride, xb, (const Mod *)c.d_mods,
+                                      (const Mod *)lv.d_bsk_mods, (const uint64_t *)lv.d_consts, lv.off, L, bsk, logn,
+                                      (uint64_t)(4 * B));
         if (e != cudaSuccess) return status_from(e);
     }
     {
@@ -428,9 +505,9 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     }
     {
         TraceScope ts("bfv_floor_sk", s);
-        behz_floor_sk_kernel<<<grid_for(3 * B * n, 256), 256, 0, s>>>(tq, tbk, out, ostride, c.d_mods, lv.d_bsk_mods,
-                                                                     lv.d_consts, lv.off, L, lv.bB, logn, 3 * B);
-        e = cudaGetLastError();
+        e = behz_dispatch<FloorLaunch>(L, 3 * B * n, s, (const uint64_t *)tq, (const uint64_t *)tbk, out, ostride,
+                                       (const Mod *)c.d_mods, (const Mod *)lv.d_bsk_mods, (const uint64_t *)lv.d_consts,
+                                       lv.off, L, lv.bB, logn, (uint64_t)(3 * B));
     }
     return e == cudaSuccess ? TB_OK : status_from(e);
 }
@@ -518,10 +595,10 @@ int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uin
     if (e != cudaSuccess) return status_from(e);
     // the lift reads polynomial p of four-polynomial groups: with both strides 4 L N
     // and b starting two polynomials in, polynomial p of x0 for every p
-    behz_lift_kernel<<<grid_for((uint64_t)P * n, 256), 256, 0, s>>>(x0, 4 * pq, x0 + 2 * pq, 4 * pq, xb, c.d_mods,
-                                                                   lv.d_bsk_mods, lv.d_consts, lv.off, L, bsk, logn,
-                                                                   (uint64_t)P);
-    e = cudaGetLastError();
+    e = behz_dispatch<LiftLaunch>(L, (uint64_t)P * n, s, (const uint64_t *)x0, 4 * pq,
+                                  (const uint64_t *)(x0 + 2 * pq), 4 * pq, xb, (const Mod *)c.d_mods,
+                                  (const Mod *)lv.d_bsk_mods, (const uint64_t *)lv.d_consts, lv.off, L, bsk, logn,
+                                  (uint64_t)P);
     if (e != cudaSuccess) return status_from(e);
     PackedNttOp<true> fb{xb, xb, lv.d_bsk_mods, bsk, logn};
     e = dispatch_ntt<true>(logn, fb, (unsigned)(P * bsk), 0, 0, s);
@@ -538,10 +615,10 @@ int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uin
     e = dispatch_ntt<false>(logn, ib, (unsigned)(D * bsk), logn, 1, s);
     if (e != cudaSuccess) return status_from(e);
     // the floor reads polynomial p = ct * 3 + poly: ostride 3 L N maps it to out + p L N
-    behz_floor_sk_kernel<<<grid_for((uint64_t)D * n, 256), 256, 0, s>>>(tq, tbk, out, 3 * pq, c.d_mods, lv.d_bsk_mods,
-                                                                       lv.d_consts, lv.off, L, lv.bB, logn,
-                                                                       (uint64_t)D);
-    return status_from(cudaGetLastError());
+    e = behz_dispatch<FloorLaunch>(L, (uint64_t)D * n, s, (const uint64_t *)tq, (const uint64_t *)tbk, out,
+                                   3 * pq, (const Mod *)c.d_mods, (const Mod *)lv.d_bsk_mods,
+                                   (const uint64_t *)lv.d_consts, lv.off, L, lv.bB, logn, (uint64_t)D);
+    return status_from(e);
 }
 
 }  // namespace tb
