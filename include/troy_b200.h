@@ -369,10 +369,12 @@ int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_st
  * (its kernels have fixed launch shapes). Settings are process-wide.
  */
 
-/* NTT launch variant for one direction and log2 block size (12..14 have variants 0, 1
-   and 2: the default thread count, half and a quarter of it, each thread taking
-   correspondingly more radix-8 groups per pass; fewer threads let several limbs share
-   an SM). */
+/* NTT launch variant for one direction and log2 block size (12..14 have variants 0 to
+   5: 0, 1 and 2 the default thread count, half and a quarter of it, each thread taking
+   correspondingly more radix-8 groups per pass, fewer threads letting several limbs
+   share an SM; 3, 4 and 5 transform a whole limb on a cluster of two CTAs holding half
+   of it each, with the thread counts of 0, 1 and 2 for the half block, and launch the
+   sub-blocks of longer limbs as 0, 1 and 2). */
 int tb_ntt_set_variant(int forward, int log_block, int variant);
 int tb_ntt_get_variant(int forward, int log_block, int *variant);
 /* Times every variant of the context's transform size on `polys` scratch limbs (0 =

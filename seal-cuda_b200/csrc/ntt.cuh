@@ -41,9 +41,13 @@ struct NttLimb {
 // most 1024 threads); variant V >= 1 divides the thread count by 2^V, each thread then
 // running more groups of a pass one after another. Fewer threads need fewer registers
 // per CTA, so several CTAs (limbs) share an SM and one CTA's barriers and memory
-// phases overlap another's arithmetic. The variant per block size is a tuning choice
-// (tb_ntt_*).
-constexpr int NTT_VARIANTS = 3;
+// phases overlap another's arithmetic. Variants 3 .. 5 transform a whole limb on a
+// cluster of two CTAs of half the block each (thread counts as variants 0 .. 2 of the
+// half block): half the shared memory per CTA, so up to twice as many limbs resident
+// per SM, for one exchange stage through distributed shared memory. Launches of a
+// sub-block of a longer limb take variant v - 3 instead. The variant per block size is
+// a tuning choice (tb_ntt_*).
+constexpr int NTT_VARIANTS = 6;
 
 template <int LOGB, int V = 0>
 struct NttCfg {
@@ -306,14 +310,14 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op
 // passes of the split transform (sub-block = cluster rank). One launch, the same
 // arithmetic and order as the split transform, and the Op's load / store see whole-
 // limb coefficient indices, so every fused operation works at this length unchanged.
-template <int LOGB, class Op>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+template <int LOGB, int V, class Op>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THREADS)
     ntt_fwd_pair_kernel(Op op) {
     namespace cg = cooperative_groups;
     extern __shared__ uint64_t sm[];
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB, 0>::THREADS;
-    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    constexpr int T = NttCfg<LOGB, V>::THREADS;
+    constexpr int REM = NttCfg<LOGB, V>::REM;
     cg::cluster_group cl = cg::this_cluster();
     const unsigned half = cl.block_rank();
     auto c = op.ctx((int)(blockIdx.x >> 1));
@@ -341,14 +345,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THR
     fwd_copy_out<NB, T>(op, c, sm, off);
 }
 
-template <int LOGB, class Op>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+template <int LOGB, int V, class Op>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THREADS)
     ntt_inv_pair_kernel(Op op) {
     namespace cg = cooperative_groups;
     extern __shared__ uint64_t sm[];
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB, 0>::THREADS;
-    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    constexpr int T = NttCfg<LOGB, V>::THREADS;
+    constexpr int REM = NttCfg<LOGB, V>::REM;
     cg::cluster_group cl = cg::this_cluster();
     const unsigned half = cl.block_rank();
     auto c = op.ctx((int)(blockIdx.x >> 1));
@@ -432,31 +436,40 @@ inline cudaError_t launch_inv(const Op &op, unsigned blocks, int logn, int scale
 // the tuner (tune.cu), read at every launch.
 int ntt_variant(bool fwd, int logb);
 
-// Whole limbs of 2^(MAX_LOGB+1) coefficients, one CTA pair each (forward from stage 0,
+// Whole limbs of 2^(LOGB+1) coefficients, one CTA pair each (forward from stage 0,
 // inverse with the N^-1 scaling).
-template <bool FWD, class Op>
+template <bool FWD, int LOGB, int V, class Op>
 inline cudaError_t launch_pair(const Op &op, unsigned blocks, cudaStream_t s) {
     if (blocks > 0x3fffffffu) return cudaErrorInvalidValue;
-    const size_t smem = ntt_smem_bytes<MAX_LOGB>();
+    const size_t smem = ntt_smem_bytes<LOGB>();
     auto k = [] {
-        if constexpr (FWD) return ntt_fwd_pair_kernel<MAX_LOGB, Op>;
-        else return ntt_inv_pair_kernel<MAX_LOGB, Op>;
+        if constexpr (FWD) return ntt_fwd_pair_kernel<LOGB, V, Op>;
+        else return ntt_inv_pair_kernel<LOGB, V, Op>;
     }();
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k<<<2 * blocks, NttCfg<MAX_LOGB, 0>::THREADS, smem, s>>>(op);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<2 * blocks, NttCfg<LOGB, V>::THREADS, smem, s>>>(op);
     return cudaGetLastError();
 }
 
 template <bool FWD, int LOGB, int V, class Op>
 inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
-    if constexpr (FWD) return launch_fwd<LOGB, V>(op, blocks, s0_or_logn, s);
-    else return launch_inv<LOGB, V>(op, blocks, s0_or_logn, scale_last, s);
+    if constexpr (V >= 3) {
+        const bool whole = FWD ? s0_or_logn == 0 : (s0_or_logn == LOGB && scale_last);
+        if (whole) return launch_pair<FWD, LOGB - 1, V - 3>(op, blocks, s);
+        return launch_ntt<FWD, LOGB, V - 3>(op, blocks, s0_or_logn, scale_last, s);
+    } else if constexpr (FWD) {
+        return launch_fwd<LOGB, V>(op, blocks, s0_or_logn, s);
+    } else {
+        return launch_inv<LOGB, V>(op, blocks, s0_or_logn, scale_last, s);
+    }
 }
 
 // Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry variants
-// with half and a quarter of the threads. 15: whole 2^15 limbs on CTA pairs (forward
-// from stage 0 only, inverse with the scaling only).
+// with half and a quarter of the threads and their CTA-pair forms. 15: whole 2^15 limbs
+// on CTA pairs (forward from stage 0 only, inverse with the scaling only).
 template <bool FWD, class Op>
 cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
 #define TB_CASE(B) \
@@ -469,6 +482,12 @@ cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn
             return launch_ntt<FWD, B, 1>(op, blocks, s0_or_logn, scale_last, s);     \
         case 2:                                                                      \
             return launch_ntt<FWD, B, 2>(op, blocks, s0_or_logn, scale_last, s);     \
+        case 3:                                                                      \
+            return launch_ntt<FWD, B, 3>(op, blocks, s0_or_logn, scale_last, s);     \
+        case 4:                                                                      \
+            return launch_ntt<FWD, B, 4>(op, blocks, s0_or_logn, scale_last, s);     \
+        case 5:                                                                      \
+            return launch_ntt<FWD, B, 5>(op, blocks, s0_or_logn, scale_last, s);     \
         default:                                                                     \
             return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);     \
         }
@@ -477,7 +496,7 @@ cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn
         TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE2(12) TB_CASE2(13) TB_CASE2(14)
     case MAX_FUSED_LOGN:
         if (FWD ? s0_or_logn != 0 : (s0_or_logn != MAX_FUSED_LOGN || !scale_last)) return cudaErrorInvalidValue;
-        return launch_pair<FWD>(op, blocks, s);
+        return launch_pair<FWD, MAX_LOGB, 0>(op, blocks, s);
     default:
         return cudaErrorInvalidValue;
     }

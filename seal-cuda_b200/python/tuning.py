@@ -14,6 +14,10 @@ import itertools
 
 import tb_capi
 
+# NTT launch variants of 2^12..2^14 blocks: 0-2 one CTA per limb at 1, 1/2, 1/4 of the
+# default thread count; 3-5 the same thread counts on a two-CTA cluster per limb
+NTT_VARIANTS = 6
+
 
 def _set(logn, fwd, inv, budget):
     lib = tb_capi.lib()
@@ -26,16 +30,17 @@ def _set(logn, fwd, inv, budget):
 
 def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
     """Times `step()` (which launches one workload step on `stream`, a torch stream)
-    under each combination of NTT variants and key-switch budget (0 = the default),
-    keeps the fastest setting and returns {"forward", "inverse", "ks_budget", "ms",
+    under candidate settings of the NTT variants and the key-switch budget (0 = the
+    default), one knob at a time (forward variant, inverse variant, budget), keeps the
+    fastest setting and returns {"forward", "inverse", "ks_budget", "ms",
     "default_ms"}."""
     import torch
 
-    variants = (0, 1, 2) if 12 <= logn <= 14 else (0,)
-    results = []
+    variants = tuple(range(NTT_VARIANTS)) if 12 <= logn <= 14 else (0,)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for fwd, inv, budget in itertools.product(variants, variants, budgets):
-        _set(logn, fwd, inv, budget)
+
+    def timed(setting):
+        _set(logn, *setting)
         step()
         torch.cuda.synchronize()
         e0.record(stream)
@@ -43,9 +48,20 @@ def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
-        results.append((e0.elapsed_time(e1) / reps, fwd, inv, budget))
-    default_ms = next(r[0] for r in results if r[1:] == (0, 0, 0))
-    ms, fwd, inv, budget = min(results)
+        return e0.elapsed_time(e1) / reps
+
+    best = (0, 0, 0)
+    default_ms = best_ms = timed(best)
+    for axis, choices in ((0, variants), (1, variants), (2, budgets)):
+        for v in choices:
+            cand = best[:axis] + (v,) + best[axis + 1:]
+            if cand == best:
+                continue
+            t = timed(cand)
+            if t < best_ms:
+                best, best_ms = cand, t
+    fwd, inv, budget = best
+    ms = best_ms
     _set(logn, fwd, inv, budget)
     return {"forward": fwd, "inverse": inv, "ks_budget": budget or "default", "ms": round(ms, 4),
             "default_ms": round(default_ms, 4)}
