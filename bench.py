@@ -63,6 +63,7 @@ METRIC = "HE mul+relin+rescale+rotate ops/s (CKKS N=16384, batched 64 pairs)"
 WORKLOAD = "ckks_n16384_L8_batch64_mul_relin_rescale_rotate"
 FALLBACK_HBM_GBS = 6650.0
 PER_OP_PAIRS = 16
+E2E_CHUNKS = 4   # sub-batches per step in the end-to-end copy pipeline
 # serving workload: encrypted vector x plaintext matrix (MatmulHelper coefficient
 # encoding), BFV N = 8192, 5 primes, 20-bit batching t, Poisson arrivals
 SERVE_N = 8192
@@ -264,42 +265,66 @@ def run_b200(args, rank, world):
     per_op_ms = e0.elapsed_time(e1) / per_op_pairs
 
     # End to end through the C ABI with host buffers: every step copies its inputs in
-    # from page-locked host memory and its results back out. The copies run on their
-    # own streams (one per direction) with two device buffer sets, so step k's inputs
-    # arrive while step k-1 computes and step k-2's results leave; events order each
-    # buffer's reuse.
+    # from page-locked host memory and its results back out. Each step's batch runs as
+    # E2E_CHUNKS sub-batches, the unit of the copy pipeline: the copies run on their own
+    # streams (one per direction) with two device buffer sets, so a sub-batch's inputs
+    # arrive while the one before computes and the one before that leaves; events order
+    # each buffer's reuse. Every pair keeps the rotation step of the batched path.
+    CH = E2E_CHUNKS if PAIRS % E2E_CHUNKS == 0 and PAIRS // E2E_CHUNKS >= len(STEPS_K) else 1
+    PC = PAIRS // CH
+    chunk_runs = []
+    for c in range(CH):
+        runs_c, at = [], 0
+        for g in range(len(STEPS_K)):
+            cnt = sum(1 for i in range(c * PC, (c + 1) * PC) if i % len(STEPS_K) == g)
+            if cnt:
+                runs_c.append((g, at, cnt))
+                at += cnt
+        chunk_runs.append(((ctypes.c_uint32 * len(runs_c))(*[elts[g] for g, _, _ in runs_c]),
+                           (ctypes.c_uint64 * len(runs_c))(*[cnt for _, _, cnt in runs_c]),
+                           (ctypes.c_void_p * len(runs_c))(*[gks[g].data_ptr() for g, _, _ in runs_c]),
+                           len(runs_c)))
+
+    def chunk_step(c, a, b, out, st=stream):
+        e_, c_, p_, nr = chunk_runs[c]
+        ctx("multiply", L, a, 0, b, 0, T3, 0, PC, st)
+        ctx("relinearize", L, T3, 0, rlk, PC, st)
+        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PC, st)
+        ctx("apply_galois_groups", L - 1, nr, e_, c_, R, 0, out, 0, p_, st)
+
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
     hO = [torch.empty(O.shape, dtype=torch.int64, pin_memory=True) for _ in range(2)]
     hA.copy_(A)
     hB.copy_(B)
-    dA = [torch.empty_like(A) for _ in range(2)]
-    dB = [torch.empty_like(B) for _ in range(2)]
-    dO = [O, torch.empty_like(O)]
+    dA = [torch.empty_like(A[:PC]) for _ in range(2)]
+    dB = [torch.empty_like(B[:PC]) for _ in range(2)]
+    dO = [torch.empty_like(O[:PC]) for _ in range(2)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
     ev = lambda: torch.cuda.Event()
     pending = {}
 
-    def e2e_step(k):
-        j = k % 2
+    def e2e_unit(u, k, c):
+        j = u % 2
+        rows = slice(c * PC, (c + 1) * PC)
         arrived, computed, left = ev(), ev(), ev()
         with torch.cuda.stream(s_in):
-            if ("computed", k - 2) in pending:
-                s_in.wait_event(pending.pop(("computed", k - 2)))   # step k-2 done reading dA[j], dB[j]
-            dA[j].copy_(hA, non_blocking=True)
-            dB[j].copy_(hB, non_blocking=True)
+            if ("computed", u - 2) in pending:
+                s_in.wait_event(pending.pop(("computed", u - 2)))   # unit u-2 done reading dA[j], dB[j]
+            dA[j].copy_(hA[rows], non_blocking=True)
+            dB[j].copy_(hB[rows], non_blocking=True)
             arrived.record(s_in)
         stream.wait_event(arrived)
-        if ("left", k - 2) in pending:
-            stream.wait_event(pending.pop(("left", k - 2)))          # dO[j] read out
-        step(dA[j], dB[j], dO[j])
+        if ("left", u - 2) in pending:
+            stream.wait_event(pending.pop(("left", u - 2)))          # dO[j] read out
+        chunk_step(c, dA[j], dB[j], dO[j])
         computed.record(stream)
         with torch.cuda.stream(s_out):
             s_out.wait_event(computed)
-            hO[j].copy_(dO[j], non_blocking=True)
+            hO[k % 2][rows].copy_(dO[j], non_blocking=True)
             left.record(s_out)
-        pending[("computed", k)] = computed
-        pending[("left", k)] = left
+        pending[("computed", u)] = computed
+        pending[("left", u)] = left
 
     def e2e_run(first, count):
         start = ev()
@@ -307,7 +332,8 @@ def run_b200(args, rank, world):
         s_in.wait_event(start)
         s_out.wait_event(start)
         for k in range(first, first + count):
-            e2e_step(k)
+            for c in range(CH):
+                e2e_unit(k * CH + c, k, c)
         for key in [key for key in pending if key[0] == "left"]:
             stream.wait_event(pending[key])                          # every result is on the host
         pending.clear()
@@ -323,7 +349,7 @@ def run_b200(args, rank, world):
     ms, e2e_ms, per_op_ms = max_over_ranks([ms, e2e_ms, per_op_ms], world, "cuda")
     return {"tuned": tuned,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
-            "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K}
+            "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH}
 
 
 def run_ntt_sweep(batch=256, reps=10):
@@ -797,7 +823,7 @@ def main():
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "l2": "inputs (256 MB) larger than L2", "tuned": res["tuned"]},
                 "e2e": {"value": round(e2e, 2), "unit": "ops/s", "h2d_bytes_per_step": res["h2d"],
-                        "d2h_bytes_per_step": res["d2h"]},
+                        "d2h_bytes_per_step": res["d2h"], "sub_batches_per_step": res["e2e_chunks"]},
                 "gpu_launches": res["launches"],
                 "roofline": roofline(res, args.steps),
                 "cpu_baseline": cpu,
