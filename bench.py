@@ -349,14 +349,17 @@ def run_b200(args, rank, world):
     ms, e2e_ms, per_op_ms = max_over_ranks([ms, e2e_ms, per_op_ms], world, "cuda")
     return {"tuned": tuned,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
-            "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH}
+            "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH,
+            "int_ceiling": int_ceiling(lib, moduli[0])}
 
 
 def run_ntt_sweep(batch=256, reps=10):
     """The raw transform workload: `batch` polynomials x 8 limbs of 50-bit primes,
     N in {4096, ..., 32768}: forward NTT, dyadic product of pairs, inverse NTT.
     Algorithmic bytes: 16 N B L per transform (read + write), 24 N B L per dyadic
-    product; GB/s and the fraction of the measured copy peak per kernel."""
+    product; GB/s and the fraction of the measured copy peak per kernel, and for the
+    transforms the fraction of the integer ceiling ((N/2) log2 N butterflies per limb
+    over tb_measure_butterfly_rate)."""
     import torch
     import tb_capi
 
@@ -367,12 +370,15 @@ def run_ntt_sweep(batch=256, reps=10):
     gen = torch.Generator(device="cuda")
     gen.manual_seed(8)
     out = {}
+    ceiling = None
     for logn in (12, 13, 14, 15):
         n = 1 << logn
         arr = (ctypes.c_int * 8)(*([50] * 8))
         mods = (ctypes.c_uint64 * 8)()
         tb_capi.check(lib.tb_coeff_modulus_create(ctypes.c_uint64(n), arr, 8, mods))
         moduli = [int(m) for m in mods]
+        if ceiling is None:
+            ceiling = int_ceiling(lib, moduli[0])
         ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
         x = _rand_residues(torch, (batch, 8, n), moduli, gen)
         y = _rand_residues(torch, (batch, 8, n), moduli, gen)
@@ -406,13 +412,17 @@ def run_ntt_sweep(batch=256, reps=10):
                                  ("ntt_inverse", ms_i, 16 * words)):
             gbs = bytes_ / (ms * 1e-3) / 1e9
             row[name] = {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4)}
+            if name != "dyadic":   # against the integer ceiling: (N/2) log2 N butterflies per limb
+                rate = batch * 8 * (n // 2) * logn / (ms * 1e-3)
+                row[name]["frac_of_int_ceiling"] = round(rate / ceiling, 4)
         row["variants"] = {"forward": vf.value, "inverse": vi.value}
         out[f"N={n}"] = row
         for fwd, v in zip((1, 0), saved):
             lib.tb_ntt_set_variant(fwd, min(logn, 14), v)
         del x, y, z
         ctx.close()
-    return {"workload": f"{batch} polynomials x 8 limbs (50-bit primes)", "results": out}
+    return {"workload": f"{batch} polynomials x 8 limbs (50-bit primes)",
+            "int_ceiling_gbutterflies_per_s": round(ceiling / 1e9, 2), "results": out}
 
 
 UNEVEN_SHAPES = [(1, 4096, [36, 36, 37]), (3, 8192, [43, 43, 44, 44, 44]), (1, 16384, [48] * 9)]
@@ -634,12 +644,45 @@ def roofline(res, steps):
     bpl = alg[name] * steps / launches
     achieved = bpl / (per_launch_ms * 1e-3) / 1e9
     tr = TRAFFIC_PER_STEP.get(name)
-    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4),
-            "traffic": round(tr * steps / launches) if tr else None,
-            "algorithmic_bytes_per_launch": round(bpl),
-            "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback",
-            "kernels": table}
+    # the transforms against the integer ceiling (butterflies per second)
+    bfly = butterflies_per_step(res["L"])
+    ceil = res.get("int_ceiling")
+    for k, row in table.items():
+        if k in bfly and ceil:
+            rate = bfly[k] / (row["ms_per_step"] * 1e-3)
+            row["int_frac"] = round(rate / ceil, 4)
+    out = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+           "frac": round(achieved / peak, 4),
+           "traffic": round(tr * steps / launches) if tr else None,
+           "algorithmic_bytes_per_launch": round(bpl),
+           "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback",
+           "kernels": table}
+    if name in bfly and ceil:
+        rate = bfly[name] * steps / launches / (per_launch_ms * 1e-3)
+        out["int"] = {"achieved": round(rate / 1e9, 2), "peak": round(ceil / 1e9, 2), "unit": "Gbutterfly/s",
+                      "frac": round(rate / ceil, 4), "butterflies_per_launch": round(bfly[name] * steps / launches),
+                      "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
+    return out
+
+
+def butterflies_per_step(L):
+    """Butterflies each traced transform kernel runs per step: (N/2) log2 N per limb
+    transformed; L data limbs at multiply/relinearize, L-1 after the rescale."""
+    per = (N // 2) * (N.bit_length() - 1)
+    B, Lr = PAIRS, L - 1
+    limbs = {"ks_target_intt": L + Lr, "ks_modup_ntt": L * L + Lr * Lr, "ks_special_intt": 2 + 2,
+             "ks_moddown": 2 * (L + Lr), "rescale_last_intt": 2, "rescale_ntt": 2 * Lr}
+    return {k: B * v * per for k, v in limbs.items()}
+
+
+def int_ceiling(lib, q):
+    """Butterflies per second of the library's lazy butterfly with everything in
+    registers (tb_measure_butterfly_rate): the integer ceiling of the transforms."""
+    lib.tb_measure_butterfly_rate.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    r = ctypes.c_double(0)
+    import tb_capi
+    tb_capi.check(lib.tb_measure_butterfly_rate(q, None, ctypes.byref(r)))
+    return r.value
 
 
 # DRAM bytes (read + write) per step of a kernel, from an ncu capture of a smaller

@@ -380,6 +380,14 @@ int tb_ntt_get_variant(int forward, int log_block, int *variant);
 /* Times every variant of the context's transform size on `polys` scratch limbs (0 =
    256) with CUDA events on `stream` and keeps the fastest per direction. */
 int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_variant, int *inverse_variant);
+/* The integer ceiling of the transforms on this device: butterflies per second of the
+   lazy Cooley-Tukey butterfly every forward NTT pass runs (Shoup product, conditional
+   subtraction, two 64-bit additions), with operands and twiddles in registers and every
+   SM at full occupancy, modulo `modulus` (odd, 3 <= modulus < 2^61). One transform of a
+   2^logn limb runs (2^logn / 2) * logn butterflies, so a transform kernel's achieved
+   rate over this one is its fraction of the integer ceiling. No counterpart in the
+   reference. */
+int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
 /* Scratch budget of one key-switch launch sequence: a batch whose intermediates exceed
    it is processed in chunks (default 2 GiB, or the TB_KS_SCRATCH_BYTES environment
    value; 0 restores the default). */

@@ -303,46 +303,43 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op
 
 // ---------------------------------------------------------------- two-CTA limbs
 // A limb of 2^(LOGB+1) coefficients transformed by a cluster of two CTAs, each holding
-// one half in shared memory. The stage whose butterflies join the halves (the first
-// forward / last inverse stage, twiddle index 1 / the N^-1-scaled pair) reads and
-// writes the partner CTA's half through distributed shared memory between two
-// cluster barriers; every other stage runs inside one half exactly as the sub-block
-// passes of the split transform (sub-block = cluster rank). One launch, the same
-// arithmetic and order as the split transform, and the Op's load / store see whole-
-// limb coefficient indices, so every fused operation works at this length unchanged.
+// one half in shared memory. Forward: the first stage (twiddle index 1) joins
+// coefficient j with j + 2^LOGB; each CTA loads both operands of its butterflies and
+// keeps the output in its own half (the first stage runs twice, once per CTA); one
+// cluster barrier before the stores keeps an in-place transform from overwriting a half
+// the partner CTA still reads. Inverse: the last stage (the N^-1-scaled pair) reads and writes the
+// partner CTA's half through distributed shared memory between two cluster barriers.
+// Every other stage runs inside one half exactly as the sub-block passes of the split
+// transform (sub-block = half). One launch, the same arithmetic and order as the split
+// transform, and the Op's load / store see whole-limb coefficient indices, so every
+// fused operation works at this length unchanged.
 template <int LOGB, int V, class Op>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THREADS)
     ntt_fwd_pair_kernel(Op op) {
-    namespace cg = cooperative_groups;
     extern __shared__ uint64_t sm[];
     constexpr int NB = 1 << LOGB;
     constexpr int T = NttCfg<LOGB, V>::THREADS;
     constexpr int REM = NttCfg<LOGB, V>::REM;
-    cg::cluster_group cl = cg::this_cluster();
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
     const unsigned half = cl.block_rank();
     auto c = op.ctx((int)(blockIdx.x >> 1));
     c.lm.sb = half;
-    const int off = (int)half << LOGB;
-    for (int e = threadIdx.x; e < NB; e += T) sm[swz(e)] = op.load(c, e + off);
-    cl.sync();
     {
-        uint64_t *lo = cl.map_shared_rank(sm, 0u), *hi = cl.map_shared_rank(sm, 1u);
         const uint64_t q = c.lm.q, q2 = q << 1;
         const ulonglong2 w = __ldg(c.lm.roots + 1);
-        for (int j = (int)half * (NB / 2) + threadIdx.x; j < (int)(half + 1) * (NB / 2); j += T) {
-            const int p = swz(j);
-            uint64_t x = lo[p], y = hi[p];
+        for (int j = threadIdx.x; j < NB; j += T) {
+            uint64_t x = op.load(c, j), y = op.load(c, j + NB);
             ct_butterfly(x, y, w, q, q2);
-            lo[p] = x;
-            hi[p] = y;
+            sm[swz(j)] = half ? y : x;
         }
     }
-    cl.sync();
+    __syncthreads();
     const uint32_t rbase = 2u + half;   // global stage 1 onwards, sub-block = half
     constexpr int FIRST = REM != 0 ? REM : 3;
     fwd_pass<FIRST, false, LOGB, T, 0, false>(op, c, sm, rbase);
     fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
-    fwd_copy_out<NB, T>(op, c, sm, off);
+    cl.sync();   // both CTAs have read every input coefficient
+    fwd_copy_out<NB, T>(op, c, sm, (int)half << LOGB);
 }
 
 template <int LOGB, int V, class Op>

@@ -103,9 +103,78 @@ int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, in
     return st;
 }
 
+// The integer ceiling of the transforms: the rate of the lazy Cooley-Tukey butterfly
+// (ct_butterfly, the one every forward NTT pass runs) with its operands and twiddles in
+// registers, so that nothing but the 64-bit modular arithmetic is timed. Each thread
+// runs the three stages of a radix-8 group (12 butterflies, 7 twiddles) `rounds` times
+// over values kept in [0, 4q); the grid fills every SM at full occupancy.
+struct Twiddles7 {
+    ulonglong2 w[7];
+};
+
+__global__ void __launch_bounds__(256) butterfly_rate_kernel(uint64_t *sink, Twiddles7 tw, uint64_t q, int rounds) {
+    const uint64_t q2 = q << 1;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = (tid * 8u + (uint32_t)k) % q;
+    for (int r = 0; r < rounds; r++) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) ct_butterfly(v[k], v[k + 4], tw.w[0], q, q2);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (!(k & 2)) ct_butterfly(v[k], v[k + 2], tw.w[1 + (k >> 2)], q, q2);
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) ct_butterfly(v[k], v[k + 1], tw.w[3 + (k >> 1)], q, q2);
+    }
+    uint64_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) x ^= v[k];
+    sink[tid] = x;
+}
+
+int measure_butterfly_rate(uint64_t q, cudaStream_t s, double *rate) {
+    if (!rate || q < 3 || !(q & 1) || q >= (1ull << 61))
+        return set_error(TB_ERR_INVALID_ARGUMENT, "modulus must be odd, at least 3 and below 2^61");
+    Twiddles7 tw;
+    uint64_t z = 0x9e3779b97f4a7c15ull ^ q;
+    for (int i = 0; i < 7; i++) {
+        z = z * 6364136223846793005ull + 1442695040888963407ull;
+        const uint64_t w = (z >> 3) % q;
+        tw.w[i] = make_ulonglong2(w, (uint64_t)(((unsigned __int128)w << 64) / q));
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, butterfly_rate_kernel, 256, 0);
+    if (e != cudaSuccess) return status_from(e);
+    const unsigned blocks = (unsigned)(sms * std::max(per_sm, 1));
+    const int rounds = 2048;
+    uint64_t *sink = nullptr;
+    e = cudaMallocAsync(&sink, 8ull * blocks * 256, s);
+    if (e != cudaSuccess) return status_from(e);
+    int st = TB_OK;
+    const float ms = time_call(
+        [&] {
+            butterfly_rate_kernel<<<blocks, 256, 0, s>>>(sink, tw, q, rounds);
+            const cudaError_t le = cudaGetLastError();
+            return le == cudaSuccess ? TB_OK : status_from(le);
+        },
+        s, 3, st);
+    cudaFreeAsync(sink, s);
+    if (st != TB_OK) return st;
+    if (!(ms > 0)) return set_error(TB_ERR_CUDA, "no timing");
+    *rate = (double)blocks * 256.0 * rounds * 12.0 / (ms * 1e-3);
+    return TB_OK;
+}
+
 }  // namespace tb
 
 extern "C" {
+
+int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second) {
+    return tb::measure_butterfly_rate(modulus, (cudaStream_t)stream, butterflies_per_second);
+}
 
 int tb_ntt_set_variant(int forward, int log_block, int variant) {
     if (log_block < 1 || log_block > tb::MAX_LOGB || variant < 0 || variant >= tb::NTT_VARIANTS ||

@@ -37,3 +37,12 @@ def test_misaligned_buffers_and_odd_strides_are_refused_on_the_host():
     assert st == 1 and b"even" in lib.tb_last_error()
     st = lib.tb_relinearize(None, 2, v(base), ctypes.c_uint64(0), v(base + 4), ctypes.c_uint64(1), None)
     assert st == 1 and b"16-byte" in lib.tb_last_error()
+
+
+def test_butterfly_rate_refuses_bad_moduli_on_the_host():
+    lib = tb_capi.lib()
+    lib.tb_measure_butterfly_rate.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    r = ctypes.c_double(0)
+    for q in (0, 2, 1 << 40, (1 << 61) + 1):
+        assert lib.tb_measure_butterfly_rate(q, None, ctypes.byref(r)) == 1
+    assert b"2^61" in lib.tb_last_error()

@@ -176,3 +176,14 @@ def test_raw_ntt_dyadic_sweep_configuration(orc, logn):
     assert torch.equal(s, torch.remainder(y + y2, torch.tensor(moduli, dtype=torch.int64, device="cuda").view(8, 1)))
     ctx("ntt_inverse", y, y, B, 0, 8, 0, None)
     assert torch.equal(y, x)
+
+
+def test_integer_ceiling_is_measured():
+    """The butterfly-rate microbenchmark runs and reports a plausible rate (between
+    1e10 and 1e14 butterflies per second on one GPU)."""
+    import ctypes
+    lib = tb_capi.lib()
+    lib.tb_measure_butterfly_rate.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    r = ctypes.c_double(0)
+    tb_capi.check(lib.tb_measure_butterfly_rate((1 << 60) - 93, None, ctypes.byref(r)))
+    assert 1e10 < r.value < 1e14
