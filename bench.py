@@ -565,12 +565,13 @@ def run_serving(seconds_per_rate=2.0, max_requests=400, pool_size=32):
             last = done if last is None else max(last, done)
         st = server.stats()
         waves = st["waves"] - waves0
-        host = {k: round(st[k] - st0[k], 4) for k in ("launch_host_s", "reap_host_s", "device_s")}
+        host = {k: round(st[k] - st0[k], 4) for k in ("launch_host_s", "alloc_host_s", "reap_host_s", "device_s")}
         return {"rate_rps": rate if rate is not None else "burst", "requests": count, "ok": ok,
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "throughput_rps": round(count / (last - first), 1), "mean_wave": round(count / max(1, waves), 2),
                 "server_seconds": host}
 
+    run(None)   # warm-up burst: the server's device pool grows to its largest wave once
     runs = [run(r) for r in SERVE_RATES] + [run(None)]
     return {"workload": "bfv_n8192_L4_matmul_poisson", "slots": 3, "memory_budget_gb": 16,
             "request_shapes": "in {64..1024} x out {16..256}, MatmulHelper coefficient encoding",

@@ -911,6 +911,7 @@ class ParmsID(list):
             d["max_wave"] = st.max_wave;
             d["launch_host_s"] = st.launch_host_s;
             d["reap_host_s"] = st.reap_host_s;
+            d["alloc_host_s"] = st.alloc_host_s;
             d["device_s"] = st.device_s;
             return d;
         });

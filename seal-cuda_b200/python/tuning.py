@@ -32,7 +32,7 @@ def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
     """Times `step()` (which launches one workload step on `stream`, a torch stream)
     under candidate settings of the NTT variants and the key-switch budget (0 = the
     default), one knob at a time (forward variant, inverse variant, budget), keeps the
-    fastest setting and returns {"forward", "inverse", "ks_budget", "ms",
+    fastest setting (a change must gain at least 1%) and returns {"forward", "inverse", "ks_budget", "ms",
     "default_ms"}."""
     import torch
 
@@ -58,7 +58,7 @@ def tune_step(step, logn, stream, reps=3, budgets=(0, 256 << 20, 8 << 30)):
             if cand == best:
                 continue
             t = timed(cand)
-            if t < best_ms:
+            if t < 0.99 * best_ms:   # a setting must beat the current one by 1% (above noise)
                 best, best_ms = cand, t
     fwd, inv, budget = best
     ms = best_ms

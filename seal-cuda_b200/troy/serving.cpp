@@ -235,7 +235,9 @@ bool MatmulServer::launch(int slot) {
     cuda_ok(cudaEventCreate(&w->begin), "event creation");
     cuda_ok(cudaEventCreate(&w->done), "event creation");
     cuda_ok(cudaEventRecord(w->begin, s), "event record");
+    const double ta = now();
     int st = cudaMallocAsync(&w->dev, total, s) == cudaSuccess ? TB_OK : TB_ERR_OUT_OF_MEMORY;
+    stats_.alloc_host_s += now() - ta;
     char *d = static_cast<char *>(w->dev);
     auto U = [&](std::size_t o) { return reinterpret_cast<uint64_t *>(d + o); };
     auto V = [&](std::size_t o) { return reinterpret_cast<const uint32_t *>(d + o); };

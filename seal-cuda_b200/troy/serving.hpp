@@ -33,6 +33,7 @@ public:
         std::uint64_t submitted = 0, completed = 0, failed = 0, waves = 0;
         std::size_t peak_bytes = 0, max_wave = 0;
         double launch_host_s = 0, reap_host_s = 0;  // host time inside launch / reap
+        double alloc_host_s = 0;                    // of launch: in the device allocator
         double device_s = 0;                        // sum of wave durations on the device
     };
 
