@@ -64,6 +64,7 @@ WORKLOAD = "ckks_n16384_L8_batch64_mul_relin_rescale_rotate"
 FALLBACK_HBM_GBS = 6650.0
 PER_OP_PAIRS = 16
 E2E_CHUNKS = 4   # sub-batches per step in the end-to-end copy pipeline
+HEADLINE_SUB_BATCHES = 4   # concurrent sub-batches (one stream each) per step of `value`
 # serving workload: encrypted vector x plaintext matrix (MatmulHelper coefficient
 # encoding), BFV N = 8192, 5 primes, 20-bit batching t, Poisson arrivals
 SERVE_N = 8192
@@ -202,11 +203,55 @@ def run_b200(args, rank, world):
     C = (ctypes.c_uint64 * len(runs))(*[cnt for _, _, cnt in runs])
     P = (ctypes.c_void_p * len(runs))(*[gks[g].data_ptr() for g, _, _ in runs])
 
-    def step(a, b, out, st=stream):
-        ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, st)
-        ctx("relinearize", L, T3, 0, rlk, PAIRS, st)
-        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, st)
-        ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, st)
+    def sub_batches(count):
+        """The batch as `count` equal sub-batches: per sub-batch its rotation runs (every
+        pair keeps the rotation step of the whole batch) as C-ABI arrays."""
+        pc = PAIRS // count
+        out = []
+        for c in range(count):
+            runs_c, at = [], 0
+            for g in range(len(STEPS_K)):
+                cnt = sum(1 for i in range(c * pc, (c + 1) * pc) if i % len(STEPS_K) == g)
+                if cnt:
+                    runs_c.append((g, at, cnt))
+                    at += cnt
+            out.append(((ctypes.c_uint32 * len(runs_c))(*[elts[g] for g, _, _ in runs_c]),
+                        (ctypes.c_uint64 * len(runs_c))(*[cnt for _, _, cnt in runs_c]),
+                        (ctypes.c_void_p * len(runs_c))(*[gks[g].data_ptr() for g, _, _ in runs_c]),
+                        len(runs_c)))
+        return pc, out
+
+    def sub_step(run_c, pc, rows, a, b, out, st):
+        e_, c_, p_, nr = run_c
+        ctx("multiply", L, a, 0, b, 0, T3[rows], 0, pc, st)
+        ctx("relinearize", L, T3[rows], 0, rlk, pc, st)
+        ctx("rescale_to_next", L, T3[rows], 3 * L * N, R[rows], 0, 2, pc, st)
+        ctx("apply_galois_groups", L - 1, nr, e_, c_, R[rows], 0, out, 0, p_, st)
+
+    # the step's batch as SUB concurrent sub-batches, one stream each (SUB = 1: the whole
+    # batch on the caller's stream): one sub-batch's short launches and wave tails
+    # overlap the other's
+    SUB = args.streams if args.streams >= 1 and PAIRS % args.streams == 0 else 1
+    sub_pc, sub_runs = sub_batches(SUB)
+    sub_streams = [torch.cuda.Stream() for _ in range(SUB)] if SUB > 1 else []
+
+    def step(a, b, out, st=stream, sub=None):
+        if (sub or SUB) == 1:
+            ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, st)
+            ctx("relinearize", L, T3, 0, rlk, PAIRS, st)
+            ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, st)
+            ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, st)
+            return
+        fork = torch.cuda.Event()
+        fork.record(st)
+        for c, sc in enumerate(sub_streams):
+            sc.wait_event(fork)
+            rows = slice(c * sub_pc, (c + 1) * sub_pc)
+            sub_step(sub_runs[c], sub_pc, rows, a[rows], b[rows], out[rows], sc)
+        for sc in sub_streams:
+            join = torch.cuda.Event()
+            join.record(sc)
+            st.wait_event(join)
 
     def barrier():
         if world > 1:
@@ -242,6 +287,18 @@ def run_b200(args, rank, world):
     lib.tb_trace_enable(0)
     trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms)) for i in range(cnt.value)}
     launches = sum(v[0] for v in trace.values()) // args.steps
+    if SUB > 1:
+        # kernels of concurrent sub-batches share the GPU, so their event times say
+        # nothing about one kernel: the per-kernel table and the roofline come from the
+        # same step as one batch on one stream (kernels alone on the GPU), timed apart
+        lib.tb_trace_enable(1)
+        for _ in range(args.steps):
+            step(A, B, O, sub=1)
+        torch.cuda.synchronize()
+        tb_capi.check(lib.tb_trace_collect(entries, 64, ctypes.byref(cnt)))
+        lib.tb_trace_enable(0)
+        trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms))
+                 for i in range(cnt.value)}
 
     # plain per-op form: one ciphertext pair per call chain (batch 1), the way the
     # reference evaluator is driven (one multiply / relinearize / rescale / rotate call
@@ -271,26 +328,10 @@ def run_b200(args, rank, world):
     # arrive while the one before computes and the one before that leaves; events order
     # each buffer's reuse. Every pair keeps the rotation step of the batched path.
     CH = E2E_CHUNKS if PAIRS % E2E_CHUNKS == 0 and PAIRS // E2E_CHUNKS >= len(STEPS_K) else 1
-    PC = PAIRS // CH
-    chunk_runs = []
-    for c in range(CH):
-        runs_c, at = [], 0
-        for g in range(len(STEPS_K)):
-            cnt = sum(1 for i in range(c * PC, (c + 1) * PC) if i % len(STEPS_K) == g)
-            if cnt:
-                runs_c.append((g, at, cnt))
-                at += cnt
-        chunk_runs.append(((ctypes.c_uint32 * len(runs_c))(*[elts[g] for g, _, _ in runs_c]),
-                           (ctypes.c_uint64 * len(runs_c))(*[cnt for _, _, cnt in runs_c]),
-                           (ctypes.c_void_p * len(runs_c))(*[gks[g].data_ptr() for g, _, _ in runs_c]),
-                           len(runs_c)))
+    PC, chunk_runs = sub_batches(CH)
 
     def chunk_step(c, a, b, out, st=stream):
-        e_, c_, p_, nr = chunk_runs[c]
-        ctx("multiply", L, a, 0, b, 0, T3, 0, PC, st)
-        ctx("relinearize", L, T3, 0, rlk, PC, st)
-        ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PC, st)
-        ctx("apply_galois_groups", L - 1, nr, e_, c_, R, 0, out, 0, p_, st)
+        sub_step(chunk_runs[c], PC, slice(0, PC), a, b, out, st)
 
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
@@ -350,7 +391,7 @@ def run_b200(args, rank, world):
     return {"tuned": tuned,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH,
-            "int_ceiling": int_ceiling(lib, moduli[0])}
+            "int_ceiling": int_ceiling(lib, moduli[0]), "sub": SUB}
 
 
 def run_ntt_sweep(batch=256, reps=10):
@@ -658,6 +699,9 @@ def roofline(res, steps):
            "algorithmic_bytes_per_launch": round(bpl),
            "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback",
            "kernels": table}
+    if res.get("sub", 1) > 1:
+        out["timing"] = (f"kernel times from the same {steps} steps run as one batch on one stream after the "
+                         f"timed region (which runs {res['sub']} concurrent sub-batches)")
     if name in bfly and ceil:
         rate = bfly[name] * steps / launches / (per_launch_ms * 1e-3)
         out["int"] = {"achieved": round(rate / 1e9, 2), "peak": round(ceil / 1e9, 2), "unit": "Gbutterfly/s",
@@ -801,6 +845,8 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
     ap.add_argument("--no-ntt-sweep", action="store_true", help="skip the raw transform sweep")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference CUDA path")
+    ap.add_argument("--streams", type=int, default=HEADLINE_SUB_BATCHES,
+                    help="concurrent sub-batches (one stream each) per step of the headline workload")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch settings (for profiler captures: no tuning launches first)")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
@@ -865,7 +911,8 @@ def main():
                 "data": "synthetic: seeded uniform residues for ciphertexts and keys",
                 "config": {"workload": WORKLOAD, "global_batch": ops_total, "seq_len": N,
                            "parallelism": "replicas" if world > 1 else "single GPU",
-                           "l2": "inputs (256 MB) larger than L2", "tuned": res["tuned"]},
+                           "l2": "inputs (256 MB) larger than L2", "tuned": res["tuned"],
+                           "concurrent_sub_batches": res["sub"]},
                 "e2e": {"value": round(e2e, 2), "unit": "ops/s", "h2d_bytes_per_step": res["h2d"],
                         "d2h_bytes_per_step": res["d2h"], "sub_batches_per_step": res["e2e_chunks"]},
                 "gpu_launches": res["launches"],
