@@ -42,6 +42,8 @@ struct RnsOff {
     int t_b;           // pair[bsk]: t mod b_k
     int inv_q_b;       // pair[bsk]: Q^-1 mod b_k
     int B_ip;          // pair[bB]: (P_B/B_k)^-1 mod B_k
+    int tq_ip;         // pair[L]: t (Q/q_i)^-1 mod q_i
+    int iqb_Bip;       // pair[bB]: Q^-1 (P_B/B_k)^-1 mod B_k
     int M_Bq;          // [L][bB]: (P_B/B_k) mod q_i
     int M_Bmsk;        // [bB]: (P_B/B_k) mod m_sk
     int inv_pb_msk;    // pair: P_B^-1 mod m_sk

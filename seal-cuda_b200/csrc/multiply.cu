@@ -66,6 +66,8 @@ int build_level_consts(Context &c, int L) {
     o.t_b = take(2 * bsk);
     o.inv_q_b = take(2 * bsk);
     o.B_ip = take(2 * bB);
+    o.tq_ip = take(2 * L);
+    o.iqb_Bip = take(2 * bB);
     o.M_Bq = take(L * bB);
     o.M_Bmsk = take(bB);
     o.inv_pb_msk = take(2);
@@ -92,6 +94,7 @@ int build_level_consts(Context &c, int L) {
         pair(o.q_ip, i, ip, q[i]);
         pair(o.q_mtip, i, mulmod(mt % q[i], ip, q[i]), q[i]);
         pair(o.t_q, i, t % q[i], q[i]);
+        pair(o.tq_ip, i, mulmod(t % q[i], ip, q[i]), q[i]);
         for (int k = 0; k < bsk; k++) h[o.M_qB + k * L + i] = punctured_mod(q, L, i, bskv[k]);
         h[o.M_qB + bsk * L + i] = punctured_mod(q, L, i, mt);
         const uint64_t pbq = prod_mod(Bv.data(), bB, q[i]);
@@ -121,6 +124,7 @@ int build_level_consts(Context &c, int L) {
         const uint64_t ip = invmod(punctured_mod(Bv.data(), bB, k, Bv[k]), Bv[k]);
         ok &= ip != 0;
         pair(o.B_ip, k, ip, Bv[k]);
+        pair(o.iqb_Bip, k, mulmod(ip, invmod(mod_words(Q, Bv[k]), Bv[k]), Bv[k]), Bv[k]);
         h[o.M_Bmsk + k] = punctured_mod(Bv.data(), bB, k, msk);
     }
     const uint64_t ipb = invmod(prod_mod(Bv.data(), bB, msk), msk);
@@ -237,11 +241,12 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
 #pragma unroll UNROLL
         for (int i = 0; i < NL; i++) {
             if (i >= L) break;
-            const uint64_t q = qm[i].value;
-            tmp[i] = pw(K, o.q_ip, i, pw(K, o.t_q, i, iq[(size_t)i << logn], q), q);
+            // t ct_i (Q/q_i)^-1 mod q_i, the two constants folded into one
+            tmp[i] = pw(K, o.tq_ip, i, iq[(size_t)i << logn], qm[i].value);
         }
-        // floor residue of Bsk prime k: (t * ct_k - conv_k(t * ct_q)) / q mod m_k
-        auto floor_residue = [&](int k) {
+        // floor residue of Bsk prime k, (t * ct_k - conv_k(t * ct_q)) / q mod m_k, times
+        // the constant at `off` (Q^-1 alone, or Q^-1 folded with the B-base factor)
+        auto floor_residue = [&](int k, int off) {
             const Mod &m = bm[k];
             U128 acc{0, 0};
 #pragma unroll UNROLL
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
             }
             const uint64_t conv = reduce128(acc.hi, acc.lo, m);
             const uint64_t bv = pw(K, o.t_b, k, ib[(size_t)k << logn], m.value);
-            return pw(K, o.inv_q_b, k, bv + m.value - conv, m.value);
+            return pw(K, off, k, bv + m.value - conv, m.value);
         };
         // Shenoy-Kumaresan: B -> q with the m_sk correction
         U128 acc_q[NL];
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
         U128 acc_sk{0, 0};
 #pragma unroll 1
         for (int k = 0; k < bB; k++) {
-            const uint64_t f = pw(K, o.B_ip, k, floor_residue(k), bm[k].value);
+            const uint64_t f = floor_residue(k, o.iqb_Bip);   // times (P_B/B_k)^-1
             mac128(acc_sk, f, K[o.M_Bmsk + k]);
 #pragma unroll UNROLL
             for (int i = 0; i < NL; i++) {
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
             }
         }
         const Mod &ms = bm[bB];
-        const uint64_t fsk = floor_residue(bB);
+        const uint64_t fsk = floor_residue(bB, o.inv_q_b);
         const uint64_t tmsk = reduce128(acc_sk.hi, acc_sk.lo, ms);
         const uint64_t alpha = mul_shoup(tmsk + (ms.value - fsk), K[o.inv_pb_msk], K[o.inv_pb_msk + 1], ms.value);
         const bool neg = alpha > (ms.value >> 1);
