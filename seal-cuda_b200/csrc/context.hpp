@@ -34,7 +34,10 @@ int set_error(int status, const std::string &msg);
 struct RnsOff {
     int q_mtip;        // pair[L]: m~ (Q/q_i)^-1 mod q_i
     int q_ip;          // pair[L]: (Q/q_i)^-1 mod q_i
-    int M_qB;          // [bsk+1][L]: (Q/q_i) mod b_k, last row mod m~
+    int M_qB;          // [bsk+1][L]: (Q/q_i) m~^-1 mod b_k (lift rows), last row (Q/q_i) mod m~
+    int M_qB_fl;       // [bsk][L]: (Q/q_i) c_k mod b_k, c_k the floor constant of b_k
+    int Qmt_b;         // pair[bsk]: Q m~^-1 mod b_k
+    int tc_b;          // pair[bsk]: t c_k mod b_k
     int neg_inv_q_mt;  // 1: -Q^-1 mod m~
     int Qmod_b;        // pair[bsk]: Q mod b_k
     int inv_mt_b;      // pair[bsk]: m~^-1 mod b_k
@@ -43,7 +46,7 @@ struct RnsOff {
     int inv_q_b;       // pair[bsk]: Q^-1 mod b_k
     int B_ip;          // pair[bB]: (P_B/B_k)^-1 mod B_k
     int tq_ip;         // pair[L]: t (Q/q_i)^-1 mod q_i
-    int iqb_Bip;       // pair[bB]: Q^-1 (P_B/B_k)^-1 mod B_k
+    int iqb_Bip;       // pair[bB]: Q^-1 (P_B/B_k)^-1 mod B_k (c_k of B_k; c of m_sk is Q^-1)
     int M_Bq;          // [L][bB]: (P_B/B_k) mod q_i
     int M_Bmsk;        // [bB]: (P_B/B_k) mod m_sk
     int inv_pb_msk;    // pair: P_B^-1 mod m_sk

@@ -59,6 +59,9 @@ int build_level_consts(Context &c, int L) {
     o.q_mtip = take(2 * L);
     o.q_ip = take(2 * L);
     o.M_qB = take((bsk + 1) * L);
+    o.M_qB_fl = take(bsk * L);
+    o.Qmt_b = take(2 * bsk);
+    o.tc_b = take(2 * bsk);
     o.neg_inv_q_mt = take(1);
     o.Qmod_b = take(2 * bsk);
     o.inv_mt_b = take(2 * bsk);
@@ -95,7 +98,6 @@ int build_level_consts(Context &c, int L) {
         pair(o.q_mtip, i, mulmod(mt % q[i], ip, q[i]), q[i]);
         pair(o.t_q, i, t % q[i], q[i]);
         pair(o.tq_ip, i, mulmod(t % q[i], ip, q[i]), q[i]);
-        for (int k = 0; k < bsk; k++) h[o.M_qB + k * L + i] = punctured_mod(q, L, i, bskv[k]);
         h[o.M_qB + bsk * L + i] = punctured_mod(q, L, i, mt);
         const uint64_t pbq = prod_mod(Bv.data(), bB, q[i]);
         pair(o.pb_q, i, pbq, q[i]);
@@ -126,6 +128,21 @@ int build_level_consts(Context &c, int L) {
         pair(o.B_ip, k, ip, Bv[k]);
         pair(o.iqb_Bip, k, mulmod(ip, invmod(mod_words(Q, Bv[k]), Bv[k]), Bv[k]), Bv[k]);
         h[o.M_Bmsk + k] = punctured_mod(Bv.data(), bB, k, msk);
+    }
+    // base-conversion rows with the constant that follows each sum folded in: the lift
+    // multiplies its result by m~^-1, the floor by c_k (Q^-1, and for B_k also the
+    // B-base factor (P_B/B_k)^-1)
+    for (int k = 0; k < bsk; k++) {
+        const uint64_t b = bskv[k];
+        const uint64_t imt = h[o.inv_mt_b + 2 * k];
+        const uint64_t ck = k < bB ? h[o.iqb_Bip + 2 * k] : h[o.inv_q_b + 2 * k];
+        for (int i = 0; i < L; i++) {
+            const uint64_t mq = punctured_mod(q, L, i, b);
+            h[o.M_qB + k * L + i] = mulmod(mq, imt, b);
+            h[o.M_qB_fl + k * L + i] = mulmod(mq, ck, b);
+        }
+        pair(o.Qmt_b, k, mulmod(h[o.Qmod_b + 2 * k], imt, b), b);
+        pair(o.tc_b, k, mulmod(t % b, ck, b), b);
     }
     const uint64_t ipb = invmod(prod_mod(Bv.data(), bB, msk), msk);
     ok &= ipb != 0;
@@ -209,10 +226,9 @@ __global__ void __launch_bounds__(256) behz_lift_kernel(const uint64_t *__restri
                 if (i >= L) break;
                 mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
             }
-            const uint64_t v = reduce128(acc.hi, acc.lo, m);
+            const uint64_t v = reduce128(acc.hi, acc.lo, m);   // already times m~^-1
             const uint64_t rr = r >= (1ull << 31) ? r + m.value - (1ull << 32) : r;
-            const uint64_t y = add_mod(pw(K, o.Qmod_b, k, rr, m.value), v, m.value);
-            out[(size_t)k << logn] = pw(K, o.inv_mt_b, k, y, m.value);
+            out[(size_t)k << logn] = add_mod(pw(K, o.Qmt_b, k, rr, m.value), v, m.value);
         }
     }
 }
@@ -244,19 +260,18 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
             // t ct_i (Q/q_i)^-1 mod q_i, the two constants folded into one
             tmp[i] = pw(K, o.tq_ip, i, iq[(size_t)i << logn], qm[i].value);
         }
-        // floor residue of Bsk prime k, (t * ct_k - conv_k(t * ct_q)) / q mod m_k, times
-        // the constant at `off` (Q^-1 alone, or Q^-1 folded with the B-base factor)
-        auto floor_residue = [&](int k, int off) {
+        // floor residue of Bsk prime k, (t * ct_k - conv_k(t * ct_q)) / q mod m_k, with
+        // the B-base factor (P_B/B_k)^-1 folded in for k < bB: c_k (t ct_k - conv_k)
+        auto floor_residue = [&](int k) {
             const Mod &m = bm[k];
             U128 acc{0, 0};
 #pragma unroll UNROLL
             for (int i = 0; i < NL; i++) {
                 if (i >= L) break;
-                mac128(acc, tmp[i], K[o.M_qB + k * L + i]);
+                mac128(acc, tmp[i], K[o.M_qB_fl + k * L + i]);
             }
-            const uint64_t conv = reduce128(acc.hi, acc.lo, m);
-            const uint64_t bv = pw(K, o.t_b, k, ib[(size_t)k << logn], m.value);
-            return pw(K, off, k, bv + m.value - conv, m.value);
+            const uint64_t conv = reduce128(acc.hi, acc.lo, m);   // c_k conv_k(t ct_q)
+            return sub_mod(pw(K, o.tc_b, k, ib[(size_t)k << logn], m.value), conv, m.value);
         };
         // Shenoy-Kumaresan: B -> q with the m_sk correction
         U128 acc_q[NL];
@@ -265,7 +280,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
         U128 acc_sk{0, 0};
 #pragma unroll 1
         for (int k = 0; k < bB; k++) {
-            const uint64_t f = floor_residue(k, o.iqb_Bip);   // times (P_B/B_k)^-1
+            const uint64_t f = floor_residue(k);   // times (P_B/B_k)^-1
             mac128(acc_sk, f, K[o.M_Bmsk + k]);
 #pragma unroll UNROLL
             for (int i = 0; i < NL; i++) {
@@ -274,7 +289,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
             }
         }
         const Mod &ms = bm[bB];
-        const uint64_t fsk = floor_residue(bB, o.inv_q_b);
+        const uint64_t fsk = floor_residue(bB);
         const uint64_t tmsk = reduce128(acc_sk.hi, acc_sk.lo, ms);
         const uint64_t alpha = mul_shoup(tmsk + (ms.value - fsk), K[o.inv_pb_msk], K[o.inv_pb_msk + 1], ms.value);
         const bool neg = alpha > (ms.value >> 1);
