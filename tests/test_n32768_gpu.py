@@ -106,3 +106,28 @@ def test_ckks_at_32768_matches_reference_words():
     want = np.roll(v * w, -1)
     assert np.abs(got - want).max() < 1e-4
     assert np.abs(got - ref.decrypt_ckks(rr, N // 2)).max() < 2.0 ** -20
+
+
+@pytest.mark.skipif(not available("ref"), reason="reference library not built")
+def test_bfv_multiply_with_more_than_16_data_limbs():
+    """17 data limbs: past the limb counts the BEHZ kernels are specialised for, the
+    run-time form gives the reference's words too."""
+    bits = [48] * 18   # 864 bits, within the 128-bit security bound at N = 32768
+    t = pytroy.PlainModulus.batching(N, 20)
+    ctx = _context(S.bfv, bits, t)
+    moduli = [m.value() for m in pytroy.CoeffModulus.create(N, bits)]
+    ref = RefSession(1, N, moduli, t.value(), np.array(SEED, np.uint64))
+    keygen = pytroy.KeyGenerator(ctx)
+    enc = pytroy.BatchEncoder(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
+    ev = pytroy.Evaluator(ctx)
+    rng = np.random.default_rng(34)
+    a = rng.integers(0, t.value(), N, dtype=np.uint64)
+    b = rng.integers(0, t.value(), N, dtype=np.uint64)
+    ea, eb = encryptor.encrypt(enc.encode(a)), encryptor.encrypt(enc.encode(b))
+    ra, rb = ref.encrypt_slots(a), ref.encrypt_slots(b)
+    m = ev.multiply(ea, eb)
+    assert _same(ref, ref.multiply(ra, rb), m)
+    dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    want = ((a.astype(object) * b.astype(object)) % t.value()).astype(np.uint64)
+    assert np.array_equal(enc.decode(dec.decrypt(m)), want)
