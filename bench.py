@@ -192,11 +192,7 @@ def run_b200(args, rank, world):
     O = torch.empty((PAIRS, 2, L - 1, N), dtype=torch.int64, device="cuda")
     # rotation groups: as many pairs per step k as pairs i with i mod 13 == g, laid out
     # in contiguous runs so each Galois key serves one batched launch
-    runs, start = [], 0
-    for g in range(len(STEPS_K)):
-        cnt = sum(1 for i in range(PAIRS) if i % len(STEPS_K) == g)
-        runs.append((g, start, cnt))
-        start += cnt
+    runs = rotation_runs(0, PAIRS, len(STEPS_K))
     words_r = 2 * (L - 1) * N
 
     E = (ctypes.c_uint32 * len(runs))(*[elts[g] for g, _, _ in runs])
@@ -209,12 +205,7 @@ def run_b200(args, rank, world):
         pc = PAIRS // count
         out = []
         for c in range(count):
-            runs_c, at = [], 0
-            for g in range(len(STEPS_K)):
-                cnt = sum(1 for i in range(c * pc, (c + 1) * pc) if i % len(STEPS_K) == g)
-                if cnt:
-                    runs_c.append((g, at, cnt))
-                    at += cnt
+            runs_c = rotation_runs(c * pc, pc, len(STEPS_K))
             out.append(((ctypes.c_uint32 * len(runs_c))(*[elts[g] for g, _, _ in runs_c]),
                         (ctypes.c_uint64 * len(runs_c))(*[cnt for _, _, cnt in runs_c]),
                         (ctypes.c_void_p * len(runs_c))(*[gks[g].data_ptr() for g, _, _ in runs_c]),
@@ -708,6 +699,19 @@ def roofline(res, steps):
                       "frac": round(rate / ceil, 4), "butterflies_per_launch": round(bfly[name] * steps / launches),
                       "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
     return out
+
+
+def rotation_runs(first, count, steps):
+    """Rotation groups of pairs first .. first + count - 1, pair i taking step i mod
+    `steps`, laid out as contiguous runs (group g, start within the sub-batch, count),
+    empty groups left out."""
+    runs, at = [], 0
+    for g in range(steps):
+        cnt = sum(1 for i in range(first, first + count) if i % steps == g)
+        if cnt:
+            runs.append((g, at, cnt))
+            at += cnt
+    return runs
 
 
 def butterflies_per_step(L):

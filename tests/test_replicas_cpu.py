@@ -52,3 +52,23 @@ def test_single_rank_is_local():
     import bench
     assert bench.max_over_ranks([1.5, 2.5], 1, "cpu") == [1.5, 2.5]
     assert bench.job_rate(64, 1, 2.0) == pytest.approx(32000.0)
+
+
+def test_sub_batches_keep_every_pairs_rotation_step():
+    """Splitting the 64-pair step into sub-batches keeps the work of the whole batch:
+    per rotation step, the sub-batches' runs count exactly the pairs that take it, and
+    each sub-batch's runs tile its pairs."""
+    import bench
+    steps, pairs = len(bench.STEPS_K), bench.DEFAULT_PAIRS
+    whole = {g: cnt for g, _, cnt in bench.rotation_runs(0, pairs, steps)}
+    assert sum(whole.values()) == pairs
+    for count in (1, 2, 4, 8):
+        pc = pairs // count
+        got = {}
+        for c in range(count):
+            runs = bench.rotation_runs(c * pc, pc, steps)
+            assert [r[1] for r in runs] == [sum(r[2] for r in runs[:k]) for k in range(len(runs))]
+            assert sum(r[2] for r in runs) == pc
+            for g, _, cnt in runs:
+                got[g] = got.get(g, 0) + cnt
+        assert got == whole
