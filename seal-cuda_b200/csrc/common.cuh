@@ -71,10 +71,13 @@ struct U128 {
     uint64_t lo, hi;
 };
 
+// acc += a * b: the low product word added with carry-out, the high word with the
+// carry-in (extended-precision multiply-add, one carry chain).
 __device__ __forceinline__ void mac128(U128 &acc, uint64_t a, uint64_t b) {
-    uint64_t lo = a * b, hi = mulhi(a, b);
-    acc.lo += lo;
-    acc.hi += hi + (acc.lo < lo);
+    asm("mad.lo.cc.u64 %0, %2, %3, %0;\n\t"
+        "madc.hi.u64 %1, %2, %3, %1;"
+        : "+l"(acc.lo), "+l"(acc.hi)
+        : "l"(a), "l"(b));
 }
 
 // Layout helper: 64-bit coefficient index -> shared-memory slot. XOR-swizzling the

@@ -162,13 +162,15 @@ __global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint6
     const Mod m = mods[mi];
     const uint64_t *__restrict__ key = keys.of((uint32_t)cb);
     U128 a00{0, 0}, a01{0, 0}, a10{0, 0}, a11{0, 0};
-    for (int j = 0; j < L; j++) {
-        const uint64_t *d = (ckks && i == j) ? target + cb * tstride + ((size_t)j << logn)
-                                             : digits + (((cb * L + j) * (L + 1) + i) << logn);
-        const ulonglong2 dv = *reinterpret_cast<const ulonglong2 *>(d + e);
-        const ulonglong2 k0 = __ldg(reinterpret_cast<const ulonglong2 *>(key + (((size_t)(2 * j) * K + mi) << logn) + e));
-        const ulonglong2 k1 =
-            __ldg(reinterpret_cast<const ulonglong2 *>(key + (((size_t)(2 * j + 1) * K + mi) << logn) + e));
+    // running pointers: digit j of output modulus i, and key digit j (polys 0 and 1) at mi
+    const size_t dstep = (size_t)(L + 1) << logn, kstep = (size_t)(2 * K) << logn, kpoly = (size_t)K << logn;
+    const uint64_t *d = digits + ((cb * L * (L + 1) + i) << logn) + e;
+    const uint64_t *k = key + ((size_t)mi << logn) + e;
+    for (int j = 0; j < L; j++, d += dstep, k += kstep) {
+        const uint64_t *dj = (ckks && i == j) ? target + cb * tstride + ((size_t)j << logn) + e : d;
+        const ulonglong2 dv = *reinterpret_cast<const ulonglong2 *>(dj);
+        const ulonglong2 k0 = __ldg(reinterpret_cast<const ulonglong2 *>(k));
+        const ulonglong2 k1 = __ldg(reinterpret_cast<const ulonglong2 *>(k + kpoly));
         mac128(a00, dv.x, k0.x);
         mac128(a01, dv.y, k0.y);
         mac128(a10, dv.x, k1.x);
