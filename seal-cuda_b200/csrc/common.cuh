@@ -51,14 +51,20 @@ __device__ __forceinline__ uint64_t reduce64(uint64_t x, const Mod &m) {
 // (hi:lo) mod q for a 128-bit value: Barrett reduction with the 128-bit ratio;
 // the truncated quotient is at most one below the true one.
 __device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo, const Mod &m) {
-    uint64_t c = mulhi(lo, m.ratio_lo);
-    uint64_t a_lo = lo * m.ratio_hi, a_hi = mulhi(lo, m.ratio_hi);
-    uint64_t t1 = a_lo + c;
-    uint64_t t3 = a_hi + (t1 < c);
-    uint64_t b_lo = hi * m.ratio_lo, b_hi = mulhi(hi, m.ratio_lo);
-    uint64_t t2 = t1 + b_lo;
-    uint64_t carry = b_hi + (t2 < t1);
-    uint64_t qt = hi * m.ratio_hi + t3 + carry;
+    // quotient estimate: the high 64 bits of (hi:lo) * (ratio_hi:ratio_lo) / 2^64 over
+    // the three partial products that reach them, carried in two multiply-add chains
+    uint64_t qt;
+    asm("{\n\t"
+        ".reg .u64 c, t1, t3, t2;\n\t"
+        "mul.hi.u64 c, %1, %3;\n\t"
+        "mad.lo.cc.u64 t1, %1, %4, c;\n\t"
+        "madc.hi.u64 t3, %1, %4, 0;\n\t"
+        "mad.lo.cc.u64 t2, %2, %3, t1;\n\t"
+        "madc.hi.u64 t3, %2, %3, t3;\n\t"
+        "mad.lo.u64 %0, %2, %4, t3;\n\t"
+        "}"
+        : "=l"(qt)
+        : "l"(lo), "l"(hi), "l"(m.ratio_lo), "l"(m.ratio_hi));
     return csub(lo - qt * m.value, m.value);
 }
 
