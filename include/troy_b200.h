@@ -377,6 +377,11 @@ int tb_negate(tb_context *ctx, int L, int size, const uint64_t *a, uint64_t a_st
    sub-blocks of longer limbs as 0, 1 and 2). */
 int tb_ntt_set_variant(int forward, int log_block, int variant);
 int tb_ntt_get_variant(int forward, int log_block, int *variant);
+/* On (the default): a launch of whole 2^12..2^14 limbs with at most half as many limbs
+   as the device has SMs takes the two-CTA form of its variant (0 -> 3, 1 -> 4, 2 -> 5),
+   so small batches (one ciphertext per call) occupy twice as many SMs; off: every launch
+   takes the set variant. */
+int tb_ntt_set_small_launch_pairs(int on);
 /* Times every variant of the context's transform size on `polys` scratch limbs (0 =
    256) with CUDA events on `stream` and keeps the fastest per direction. */
 int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_variant, int *inverse_variant);

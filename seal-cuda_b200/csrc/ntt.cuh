@@ -432,6 +432,10 @@ inline cudaError_t launch_inv(const Op &op, unsigned blocks, int logn, int scale
 // Tuned thread-count variant per (direction, log2 block size); 0 = default. Written by
 // the tuner (tune.cu), read at every launch.
 int ntt_variant(bool fwd, int logb);
+// Streaming multiprocessors of the current device (cached per device).
+int sm_count();
+// Whether launches of fewer limbs than SMs take the two-CTA form (tb_ntt_set_small_launch_pairs).
+bool small_launch_pairs();
 
 // Whole limbs of 2^(LOGB+1) coefficients, one CTA pair each (forward from stage 0,
 // inverse with the N^-1 scaling).
@@ -464,6 +468,16 @@ inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int
     }
 }
 
+// A launch of at most half as many limbs as the device has SMs leaves most SMs idle with
+// one CTA per limb: it takes the two-CTA form of the same thread count, which puts twice
+// as many CTAs to work (one pair per call chain, as the reference drives the evaluator:
+// +43% ops/s at N = 16384). Larger launches keep the tuned variant (nearer a full wave
+// the one-CTA form is faster: the pair form exchanges a stage through distributed
+// shared memory or loads its limb twice).
+inline int small_launch_variant(int v, unsigned blocks) {
+    return (v < 3 && small_launch_pairs() && 2 * blocks <= (unsigned)sm_count()) ? v + 3 : v;
+}
+
 // Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry variants
 // with half and a quarter of the threads and their CTA-pair forms. 15: whole 2^15 limbs
 // on CTA pairs (forward from stage 0 only, inverse with the scaling only).
@@ -474,7 +488,7 @@ cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn
         return launch_ntt<FWD, B, 0>(op, blocks, s0_or_logn, scale_last, s);
 #define TB_CASE2(B)                                                                  \
     case B:                                                                          \
-        switch (ntt_variant(FWD, B)) {                                               \
+        switch (small_launch_variant(ntt_variant(FWD, B), blocks)) {                 \
         case 1:                                                                      \
             return launch_ntt<FWD, B, 1>(op, blocks, s0_or_logn, scale_last, s);     \
         case 2:                                                                      \

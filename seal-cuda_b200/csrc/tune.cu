@@ -19,7 +19,21 @@ namespace tb {
 namespace {
 std::atomic<int> g_variant[2][MAX_LOGB + 1];
 std::atomic<unsigned long long> g_ks_budget{0};
+std::atomic<int> g_small_pairs{1};
 }  // namespace
+
+bool small_launch_pairs() { return g_small_pairs.load(std::memory_order_relaxed) != 0; }
+
+int sm_count() {
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) return 148;
+    cached[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
 
 int ntt_variant(bool fwd, int logb) {
     if (logb < 0 || logb > MAX_LOGB) return 0;
@@ -187,6 +201,11 @@ int tb_ntt_set_variant(int forward, int log_block, int variant) {
 int tb_ntt_get_variant(int forward, int log_block, int *variant) {
     if (!variant || log_block < 1 || log_block > tb::MAX_LOGB) return tb::set_error(TB_ERR_INVALID_ARGUMENT, "bad block");
     *variant = tb::ntt_variant(forward != 0, log_block);
+    return TB_OK;
+}
+
+int tb_ntt_set_small_launch_pairs(int on) {
+    tb::g_small_pairs.store(on != 0);
     return TB_OK;
 }
 

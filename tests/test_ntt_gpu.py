@@ -112,6 +112,7 @@ def test_ntt_launch_variants_are_identical(orc, logn):
     exp_f = orc.ntt_forward_rns(logn, moduli, x, lazy=False)
     exp_i = orc.ntt_inverse_rns(logn, moduli, x, lazy=False)
     try:
+        tb_capi.check(lib.tb_ntt_set_small_launch_pairs(0))   # every launch takes the set variant
         for v in range(6):
             for b in (12, 13, 14):
                 tb_capi.check(lib.tb_ntt_set_variant(1, b, v))
@@ -127,6 +128,7 @@ def test_ntt_launch_variants_are_identical(orc, logn):
         ctx("ntt_forward", d, out, 1, 0, len(moduli), 0, None)
         assert np.array_equal(_host(out), exp_f)
     finally:
+        lib.tb_ntt_set_small_launch_pairs(1)
         for b in (12, 13, 14):
             lib.tb_ntt_set_variant(1, b, 0)
             lib.tb_ntt_set_variant(0, b, 0)

@@ -1,6 +1,7 @@
-"""Every NTT launch variant inside the fused operations: with variants 0..5 set for the
-ring degree's block size (one CTA or a two-CTA cluster per limb, three thread counts
-each), seeded BFV and CKKS chains (encrypt, multiply, relinearize, rotate, mod-switch /
+"""Every NTT launch variant inside the fused operations: with variants 0..5 forced for
+the ring degree's block size (one CTA or a two-CTA cluster per limb, three thread counts
+each), and with the default (variant 0, launches smaller than the SM count on CTA
+pairs), seeded BFV and CKKS chains (encrypt, multiply, relinearize, rotate, mod-switch /
 rescale) give the reference CPU path's words at every step."""
 import numpy as np
 import pytest
@@ -34,13 +35,19 @@ def _context(scheme, n, bits, t=None):
 
 
 def _set_variant(logn, v):
+    """Variant v for every launch (the small-launch rule off); v = None restores the
+    default: variant 0 with small launches on CTA pairs."""
     lib = tb_capi.lib()
-    tb_capi.check(lib.tb_ntt_set_variant(1, logn, v))
-    tb_capi.check(lib.tb_ntt_set_variant(0, logn, v))
+    tb_capi.check(lib.tb_ntt_set_variant(1, logn, v or 0))
+    tb_capi.check(lib.tb_ntt_set_variant(0, logn, v or 0))
+    tb_capi.check(lib.tb_ntt_set_small_launch_pairs(1 if v is None else 0))
+
+
+VARIANTS = list(range(6)) + [None]
 
 
 @pytest.mark.skipif(not available("ref"), reason="reference library not built")
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", VARIANTS)
 def test_bfv_chain_under_each_variant(variant):
     n, bits = 8192, [50, 50, 50, 50]
     t = pytroy.PlainModulus.batching(n, 20)
@@ -53,7 +60,7 @@ def test_bfv_chain_under_each_variant(variant):
     enc = pytroy.BatchEncoder(ctx)
     encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
     ev = pytroy.Evaluator(ctx)
-    rng = np.random.default_rng(40 + variant)
+    rng = np.random.default_rng(40 + (variant or 0))
     a = rng.integers(0, t.value(), n, dtype=np.uint64)
     b = rng.integers(0, t.value(), n, dtype=np.uint64)
     ra, rb = ref.encrypt_slots(a), ref.encrypt_slots(b)
@@ -73,11 +80,11 @@ def test_bfv_chain_under_each_variant(variant):
         ms = ev.mod_switch_to_next(r)
         assert _same(ref, ref.mod_switch(rr), ms)
     finally:
-        _set_variant(13, 0)
+        _set_variant(13, None)
 
 
 @pytest.mark.skipif(not available("ref"), reason="reference library not built")
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", VARIANTS)
 def test_ckks_chain_under_each_variant(variant):
     n, bits, scale = 16384, [60] + [40] * 5 + [60], 2.0 ** 40
     ctx = _context(S.ckks, n, bits)
@@ -88,7 +95,7 @@ def test_ckks_chain_under_each_variant(variant):
     enc = pytroy.CKKSEncoder(ctx)
     encryptor = pytroy.Encryptor(ctx, keygen.create_public_key())
     ev = pytroy.Evaluator(ctx)
-    rng = np.random.default_rng(50 + variant)
+    rng = np.random.default_rng(50 + (variant or 0))
     v = rng.uniform(-1, 1, n // 2) + 1j * rng.uniform(-1, 1, n // 2)
     w = rng.uniform(-1, 1, n // 2) + 1j * rng.uniform(-1, 1, n // 2)
     ra, rb = ref.encrypt_ckks(v, scale), ref.encrypt_ckks(w, scale)
@@ -110,4 +117,4 @@ def test_ckks_chain_under_each_variant(variant):
         got = enc.decode(pytroy.Decryptor(ctx, keygen.secret_key()).decrypt(r))
         assert np.abs(got - np.roll(v * w, -1)).max() < 1e-4
     finally:
-        _set_variant(14, 0)
+        _set_variant(14, None)
