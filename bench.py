@@ -1,6 +1,6 @@
 """Benchmark of the ciphertext-arithmetic hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--streams S]
 
 Workload (the batched CKKS evaluation the headline metric is quoted on):
 CKKS, N = 16384, coefficient modulus chain {60, 40 x 7, 60} bits (8 data limbs and
@@ -11,12 +11,15 @@ that chain. Inputs and keys are seeded, uniformly random residues modulo each
 prime (the arithmetic performed is the same as on encrypted data).
 
 * ``value``: ops/s with inputs resident in HBM (CUDA events on the launch stream,
-  max over ranks). Inputs (2 x 128 MB) exceed the 126 MB L2 between steps.
+  max over ranks). Inputs (2 x 128 MB) exceed the 126 MB L2 between steps. Each
+  step's 64 pairs run as S concurrent sub-batches, one stream each (default 4).
 * ``e2e``: the same metric through the C ABI with host buffers: every step copies
-  both operand batches from pinned host memory and reads the results back; the
-  copies run on one stream per direction, overlapping the neighbouring steps'
-  arithmetic (two device buffer sets, ordered by events).
-* ``roofline``: the dominant kernel from the library's per-launch event trace.
+  both operand batches from pinned host memory and reads the results back, as 4
+  sub-batches whose copies run on one stream per direction, overlapping the
+  neighbouring sub-batches' arithmetic (two device buffer sets, ordered by events).
+* ``roofline``: the dominant kernel from the library's per-launch event trace of the
+  same steps run as one batch on one stream, against the measured HBM copy peak and
+  (``roofline.int``) the measured integer ceiling of the transforms.
 * ``cpu_baseline``: the reference's own CPU implementation (compiled under
   oracle/_ref) on a bounded sample of the same workload, one process per core.
 * ``plain_per_op``: the same chain driven one pair per call (batch 1), as the
@@ -25,7 +28,8 @@ prime (the arithmetic performed is the same as on encrypted data).
   for sm_100a under oracle/_ref by oracle/Makefile) on the same workload, one pair
   per call, in a child process; ``batched_over_reference_gpu_per_op`` compares.
 * ``ntt_sweep``: the raw NTT / dyadic / inverse NTT workload (256 x 8 limbs, N =
-  4096 .. 32768) with GB/s and fraction of the measured copy peak per kernel.
+  4096 .. 32768) with GB/s and fraction of the measured copy peak per kernel, and of
+  the integer ceiling per transform.
 * ``uneven_batch``: 512 BFV/BGV ciphertexts of degrees 4096 / 8192 / 16384 through
   multiply, relinearize and rotate_rows as one captured CUDA graph, beside the
   one-ciphertext-per-call path.
