@@ -192,7 +192,7 @@ __device__ __forceinline__ uint64_t pw(const uint64_t *K, int off, int i, uint64
 // inputs of B products: polynomial p = ct*4 + slot, slots 0,1 from a and 2,3 from b;
 // output [B][4][bsk][N].
 template <int LT>
-__global__ void __launch_bounds__(256) behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astride,
+__global__ void __launch_bounds__(256, 3) behz_lift_kernel(const uint64_t *__restrict__ a, uint64_t astride,
                                                         const uint64_t *__restrict__ b, uint64_t bstride,
                                                         uint64_t *__restrict__ dst, const Mod *__restrict__ qm,
                                                         const Mod *__restrict__ bm, const uint64_t *__restrict__ K,
