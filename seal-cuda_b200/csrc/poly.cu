@@ -12,7 +12,8 @@ __global__ void dyadic_kernel(const uint64_t *__restrict__ a, const uint64_t *__
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total_pairs;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t e = i * 2;
-        const int l = (int)((e >> logn) % limbs);
+        // limb of the coefficient: a 32-bit remainder (polynomial-limb indices fit 32 bits)
+        const int l = (int)((uint32_t)(e >> logn) % (uint32_t)limbs);
         const Mod m = mods[first + l];
         const ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + e);
         const ulonglong2 y = *reinterpret_cast<const ulonglong2 *>(b + e);
@@ -62,8 +63,18 @@ __global__ void tensor_kernel(const uint64_t *__restrict__ a, uint64_t astride, 
     const uint64_t per = (uint64_t)L << (logn - 1);  // coefficient pairs per polynomial
     const uint64_t total = B * per;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t cb = i / per;
-        const uint64_t w = (i - cb * per) * 2;   // word offset inside a polynomial
+        // ciphertext and word offset inside its polynomial: one 32-bit division by the
+        // limb count (i >> (logn - 1) counts whole limbs) where the index fits 32 bits
+        uint64_t cb, w;
+        if (total <= 0xffffffffull) {
+            const uint32_t limb_idx = (uint32_t)i >> (logn - 1);
+            const uint32_t c32 = limb_idx / (uint32_t)L;
+            cb = c32;
+            w = ((uint64_t)(limb_idx - c32 * (uint32_t)L) << logn) + ((i & ((1ull << (logn - 1)) - 1)) << 1);
+        } else {
+            cb = i / per;
+            w = (i - cb * per) * 2;
+        }
         const int l = (int)(w >> logn);
         const Mod m = mods[first + l];
         const uint64_t pl = (uint64_t)L << logn;
