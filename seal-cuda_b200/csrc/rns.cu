@@ -155,8 +155,18 @@ __global__ void mod_switch_coeff_kernel(const uint64_t *__restrict__ in, uint64_
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t p = i >> logn;
         const uint32_t e = (uint32_t)(i & (n - 1));
-        const uint64_t *src = in + (p / size) * istride + (((p % size) * L) << logn);
-        uint64_t *dst = out + (p / size) * ostride + (((p % size) * (L - 1)) << logn);
+        // ciphertext and polynomial of p: a 32-bit division where the count fits 32 bits
+        uint64_t pc, pk;
+        if (P <= 0xffffffffull) {
+            const uint32_t c32 = (uint32_t)p / (uint32_t)size;
+            pc = c32;
+            pk = (uint32_t)p - c32 * (uint32_t)size;
+        } else {
+            pc = p / size;
+            pk = p % size;
+        }
+        const uint64_t *src = in + pc * istride + ((pk * L) << logn);
+        uint64_t *dst = out + pc * ostride + ((pk * (L - 1)) << logn);
         const Mod ml = mods[L - 1];
         const uint64_t ql = ml.value;
         const uint64_t last = src[((size_t)(L - 1) << logn) + e];
