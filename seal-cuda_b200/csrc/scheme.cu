@@ -90,6 +90,26 @@ cudaError_t transform(const Context &c, uint64_t *buf, uint64_t polys, int first
 
 // ---------------------------------------------------------------- element-wise
 
+// Index w of a limb-major layout split by units of d limbs of 2^logn words:
+// (w / (d << logn), w mod (d << logn)), with a 32-bit division where the limb index fits.
+__device__ __forceinline__ void split_limbs(uint64_t w, uint32_t d, int logn, uint64_t &q, uint64_t &r) {
+    const uint64_t limb = w >> logn, low = w & ((1ull << logn) - 1);
+    if (limb <= 0xffffffffull) {
+        const uint32_t l32 = (uint32_t)limb, q32 = l32 / d;
+        q = q32;
+        r = ((uint64_t)(l32 - q32 * d) << logn) | low;
+    } else {
+        q = limb / d;
+        r = ((limb - q * d) << logn) | low;
+    }
+}
+
+// Limb of a limb-major index: (w >> logn) mod L, a 32-bit remainder where it fits.
+__device__ __forceinline__ int limb_of(uint64_t w, int logn, int L) {
+    const uint64_t limb = w >> logn;
+    return limb <= 0xffffffffull ? (int)((uint32_t)limb % (uint32_t)L) : (int)(limb % (uint64_t)L);
+}
+
 // out[p][l] = a[p][l] (*) b[pb][l] with pb = p / bdiv (broadcast b over ciphertexts).
 __global__ void dyadic_bcast_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b,
                                     uint64_t *__restrict__ out, const Mod *__restrict__ mods, int L, int logn,
@@ -97,9 +117,11 @@ __global__ void dyadic_bcast_kernel(const uint64_t *__restrict__ a, const uint64
     const uint64_t per = (uint64_t)L << logn;
     const uint64_t total = P * per;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t p = w / per, r = w - p * per;
+        uint64_t p, r;
+        split_limbs(w, (uint32_t)L, logn, p, r);
         const int l = (int)(r >> logn);
-        const uint64_t bi = (p / bdiv) * bstride_poly + r;
+        const uint64_t pb = (p <= 0xffffffffull && bdiv <= 0xffffffffull) ? (uint32_t)p / (uint32_t)bdiv : p / bdiv;
+        const uint64_t bi = pb * bstride_poly + r;
         out[w] = mul_mod(a[w], b[bi], mods[l]);
     }
 }
@@ -111,8 +133,9 @@ __global__ void addsub_kernel(const uint64_t *__restrict__ a, uint64_t astride, 
     const uint64_t per = (uint64_t)size * L << logn;
     const uint64_t total = B * per;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t cb = w / per, r = w - cb * per;
-        const int l = (int)((r >> logn) % L);
+        uint64_t cb, r;
+        split_limbs(w, (uint32_t)size * (uint32_t)L, logn, cb, r);
+        const int l = limb_of(r, logn, L);
         const uint64_t q = mods[l].value;
         const uint64_t x = a[cb * astride + r];
         uint64_t y;
@@ -127,8 +150,7 @@ __global__ void addsub_kernel(const uint64_t *__restrict__ a, uint64_t astride, 
 __global__ void add_noise_kernel(uint64_t *__restrict__ x, const uint64_t *__restrict__ e, const Mod *__restrict__ mods,
                                  int L, int logn, uint64_t total, uint64_t t_scale) {
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
-        const int l = (int)((w >> logn) % L);
-        const Mod m = mods[l];
+        const Mod m = mods[limb_of(w, logn, L)];
         uint64_t v = e[w];
         if (t_scale) v = mul_mod(v, reduce64(t_scale, m), m);
         x[w] = add_mod(x[w], v, m.value);
@@ -159,7 +181,8 @@ __global__ void add_plain_kernel(uint64_t *__restrict__ ct, uint64_t cstride, co
     const uint32_t n = 1u << logn;
     const uint64_t total = B * (uint64_t)L * n;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = w / ((uint64_t)L * n), r = w - b * (uint64_t)L * n;
+        uint64_t b, r;
+        split_limbs(w, (uint32_t)L, logn, b, r);
         const int l = (int)(r >> logn);
         const uint32_t i = (uint32_t)(r & (n - 1));
         const Mod m = mods[l];
