@@ -5,8 +5,11 @@
 Workload (the batched CKKS evaluation the headline metric is quoted on):
 CKKS, N = 16384, coefficient modulus chain {60, 40 x 7, 60} bits (8 data limbs and
 one special prime), 64 ciphertext pairs per step. Each pair goes through
-multiply -> relinearize -> rescale_to_next -> rotate_vector(k), k = 2^(i mod 13)
-for pair i (13 Galois keys, k in {1, 2, 4, ..., 4096}). One op = one pair through
+multiply -> relinearize -> rescale_to_next -> rotate_vector(k) over 13 Galois keys,
+k in {1, 2, 4, ..., 4096}, each step taken by as many pairs as pairs i with
+i mod 13 == log2 k (the pairs of a step consecutive inside each sub-batch, so one
+grouped Galois call serves all 13 keys; seal-cuda_b200/python/ckks_step.py, the
+same step the GPU parity test checks word for word). One op = one pair through
 that chain. Inputs and keys are seeded, uniformly random residues modulo each
 prime (the arithmetic performed is the same as on encrypted data).
 
@@ -164,6 +167,7 @@ def _rand_residues(torch, shape, moduli, gen):
 
 def run_b200(args, rank, world):
     import torch
+    import ckks_step
     import tb_capi
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -191,62 +195,18 @@ def run_b200(args, rank, world):
     # operands
     A = _rand_residues(torch, (PAIRS, 2, L, N), moduli[:L], gen)
     B = _rand_residues(torch, (PAIRS, 2, L, N), moduli[:L], gen)
-    T3 = torch.empty((PAIRS, 3, L, N), dtype=torch.int64, device="cuda")
-    R = torch.empty((PAIRS, 2, L - 1, N), dtype=torch.int64, device="cuda")
     O = torch.empty((PAIRS, 2, L - 1, N), dtype=torch.int64, device="cuda")
-    # rotation groups: as many pairs per step k as pairs i with i mod 13 == g, laid out
-    # in contiguous runs so each Galois key serves one batched launch
-    runs = rotation_runs(0, PAIRS, len(STEPS_K))
-    words_r = 2 * (L - 1) * N
-
-    E = (ctypes.c_uint32 * len(runs))(*[elts[g] for g, _, _ in runs])
-    C = (ctypes.c_uint64 * len(runs))(*[cnt for _, _, cnt in runs])
-    P = (ctypes.c_void_p * len(runs))(*[gks[g].data_ptr() for g, _, _ in runs])
-
-    def sub_batches(count):
-        """The batch as `count` equal sub-batches: per sub-batch its rotation runs (every
-        pair keeps the rotation step of the whole batch) as C-ABI arrays."""
-        pc = PAIRS // count
-        out = []
-        for c in range(count):
-            runs_c = rotation_runs(c * pc, pc, len(STEPS_K))
-            out.append(((ctypes.c_uint32 * len(runs_c))(*[elts[g] for g, _, _ in runs_c]),
-                        (ctypes.c_uint64 * len(runs_c))(*[cnt for _, _, cnt in runs_c]),
-                        (ctypes.c_void_p * len(runs_c))(*[gks[g].data_ptr() for g, _, _ in runs_c]),
-                        len(runs_c)))
-        return pc, out
-
-    def sub_step(run_c, pc, rows, a, b, out, st):
-        e_, c_, p_, nr = run_c
-        ctx("multiply", L, a, 0, b, 0, T3[rows], 0, pc, st)
-        ctx("relinearize", L, T3[rows], 0, rlk, pc, st)
-        ctx("rescale_to_next", L, T3[rows], 3 * L * N, R[rows], 0, 2, pc, st)
-        ctx("apply_galois_groups", L - 1, nr, e_, c_, R[rows], 0, out, 0, p_, st)
-
     # the step's batch as SUB concurrent sub-batches, one stream each (SUB = 1: the whole
     # batch on the caller's stream): one sub-batch's short launches and wave tails
-    # overlap the other's
+    # overlap the other's. Inside a sub-batch the pairs of each rotation step are
+    # consecutive, so one grouped Galois call serves all 13 keys.
     SUB = args.streams if args.streams >= 1 and PAIRS % args.streams == 0 else 1
-    sub_pc, sub_runs = sub_batches(SUB)
-    sub_streams = [torch.cuda.Stream() for _ in range(SUB)] if SUB > 1 else []
+    stepper = ckks_step.BatchedCkksStep(torch, ctx, L, N, PAIRS, rlk, elts, gks, SUB)
+    T3 = stepper.T3
+    R = stepper.R
 
     def step(a, b, out, st=stream, sub=None):
-        if (sub or SUB) == 1:
-            ctx("multiply", L, a, 0, b, 0, T3, 0, PAIRS, st)
-            ctx("relinearize", L, T3, 0, rlk, PAIRS, st)
-            ctx("rescale_to_next", L, T3, 3 * L * N, R, 0, 2, PAIRS, st)
-            ctx("apply_galois_groups", L - 1, len(runs), E, C, R, 0, out, 0, P, st)
-            return
-        fork = torch.cuda.Event()
-        fork.record(st)
-        for c, sc in enumerate(sub_streams):
-            sc.wait_event(fork)
-            rows = slice(c * sub_pc, (c + 1) * sub_pc)
-            sub_step(sub_runs[c], sub_pc, rows, a[rows], b[rows], out[rows], sc)
-        for sc in sub_streams:
-            join = torch.cuda.Event()
-            join.record(sc)
-            st.wait_event(join)
+        stepper(a, b, out, st, sub)
 
     def barrier():
         if world > 1:
@@ -323,10 +283,11 @@ def run_b200(args, rank, world):
     # arrive while the one before computes and the one before that leaves; events order
     # each buffer's reuse. Every pair keeps the rotation step of the batched path.
     CH = E2E_CHUNKS if PAIRS % E2E_CHUNKS == 0 and PAIRS // E2E_CHUNKS >= len(STEPS_K) else 1
-    PC, chunk_runs = sub_batches(CH)
+    PC = PAIRS // CH
+    chunk_runs = [stepper.runs(c * PC, PC) for c in range(CH)]
 
     def chunk_step(c, a, b, out, st=stream):
-        sub_step(chunk_runs[c], PC, slice(0, PC), a, b, out, st)
+        stepper.chain(chunk_runs[c], PC, slice(0, PC), a, b, out, st)
 
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
@@ -680,7 +641,7 @@ def roofline(res, steps):
     per_launch_ms = total_ms / launches
     bpl = alg[name] * steps / launches
     achieved = bpl / (per_launch_ms * 1e-3) / 1e9
-    tr = TRAFFIC_PER_STEP.get(name)
+    tr = measured_traffic().get(name)
     # the transforms against the integer ceiling (butterflies per second)
     bfly = butterflies_per_step(res["L"])
     ceil = res.get("int_ceiling")
@@ -688,9 +649,17 @@ def roofline(res, steps):
         if k in bfly and ceil:
             rate = bfly[k] / (row["ms_per_step"] * 1e-3)
             row["int_frac"] = round(rate / ceil, 4)
-    out = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+    # the bound is the resource the kernel uses the larger fraction of: HBM bandwidth, or
+    # the integer ceiling of the transforms
+    int_frac = None
+    if name in bfly and ceil:
+        int_frac = bfly[name] * steps / launches / (per_launch_ms * 1e-3) / ceil
+    bound = "int" if int_frac is not None and int_frac > achieved / peak else "hbm"
+    out = {"kernel": name, "bound": bound, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
            "frac": round(achieved / peak, 4),
            "traffic": round(tr * steps / launches) if tr else None,
+           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel at this shape "
+                             "(profiles/ckks_step_n16384_traffic.md), per launch" if tr else None,
            "algorithmic_bytes_per_launch": round(bpl),
            "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "of fallback",
            "kernels": table}
@@ -703,19 +672,6 @@ def roofline(res, steps):
                       "frac": round(rate / ceil, 4), "butterflies_per_launch": round(bfly[name] * steps / launches),
                       "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
     return out
-
-
-def rotation_runs(first, count, steps):
-    """Rotation groups of pairs first .. first + count - 1, pair i taking step i mod
-    `steps`, laid out as contiguous runs (group g, start within the sub-batch, count),
-    empty groups left out."""
-    runs, at = [], 0
-    for g in range(steps):
-        cnt = sum(1 for i in range(first, first + count) if i % steps == g)
-        if cnt:
-            runs.append((g, at, cnt))
-            at += cnt
-    return runs
 
 
 def butterflies_per_step(L):
@@ -738,11 +694,21 @@ def int_ceiling(lib, q):
     return r.value
 
 
-# DRAM bytes (read + write) per step of a kernel, from an ncu capture of a smaller
-# batch of this workload scaled by the units processed: the mod-up launch at L = 8 of
-# 16 ciphertexts moved 19.268608 + 75.146240 MB; a step runs it for 64 ciphertexts at
-# L = 8 (x4) and at L = 7 (x4 x (7 + 49) / (8 + 64) target limbs and digits).
-TRAFFIC_PER_STEP: dict = {"ks_modup_ntt": (19.268608e6 + 75.146240e6) * 4 * (1 + 56 / 72)}
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "ckks_step_n16384_traffic.md")
+
+
+def measured_traffic():
+    """DRAM bytes (read + write) per step of each kernel of the one-stream step at the
+    benchmark's shape (64 pairs, L = 8 and 7), from the ncu capture summarised in
+    profiles/ckks_step_n16384_traffic.md (its json block: kernel -> bytes per step);
+    {} when the summary is absent."""
+    try:
+        with open(TRAFFIC_PROFILE) as f:
+            text = f.read()
+        block = text.split("```json", 1)[1].split("```", 1)[0]
+        return {k: float(v) for k, v in json.loads(block)["bytes_per_step"].items()}
+    except (OSError, IndexError, KeyError, ValueError):
+        return {}
 
 
 # -------------------------------------------------------------- CPU baseline
@@ -832,6 +798,18 @@ def reference_gpu_per_op(ops=16):
             else "reference EvaluatorCuda compiled for sm_100a"}
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def _cpu_count():
     try:
         return len(os.sched_getaffinity(0))
@@ -847,7 +825,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker in the baseline sample")
+    ap.add_argument("--cpu-ops", type=int, default=16, help="ops per CPU worker per step of --impl reference")
+    ap.add_argument("--cpu-baseline-ops", type=int, default=128,
+                    help="ops per CPU worker in the cpu_baseline sample of the GPU arm (about 10 - 20 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
@@ -882,6 +862,7 @@ def main():
                 "config": {"workload": WORKLOAD, "global_batch": args.cpu_ops * workers, "seq_len": N,
                            "parallelism": f"{workers} CPU processes"},
                 "cpu_baseline": {"value": round(value, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
+                                 "cpu_model": _cpu_model(),
                                  "sample": f"{args.cpu_ops} ops per process x {workers} processes per step"},
                 "e2e": {"value": round(value, 3), "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -903,9 +884,11 @@ def main():
         cpu = None
         if not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libtroyref.so")):
             workers = min(cores, 32)
-            v, ops, busy, wall = cpu_reference(args.cpu_ops, workers)
+            v, ops, busy, wall = cpu_reference(args.cpu_baseline_ops, workers)
             cpu = {"value": round(v, 3), "unit": "ops/s", "cores": workers, "kind": "reference",
-                   "sample": f"{ops} ops ({args.cpu_ops} per process x {workers} processes), {busy:.1f} s"}
+                   "cpu_model": _cpu_model(),
+                   "sample": f"{ops} ops ({args.cpu_baseline_ops} per process x {workers} processes), "
+                             f"{busy:.1f} s"}
         per_op = 1e3 / res["per_op_ms"]
         ref_gpu = None if args.no_reference_gpu else reference_gpu_per_op()
         if ref_gpu and "value" in ref_gpu:

@@ -160,10 +160,11 @@ int tb_relinearize(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, con
  * calls no allocator: it works out of a 16 MiB scratch array in the library's device
  * image (held on every GPU that loads the library until exit), one chunk of the
  * batch at a time. A level whose single-ciphertext scratch exceeds 16 MiB is
- * rejected with TB_ERR_INVALID_ARGUMENT (e.g. CKKS N=16384 fits up to L=8). The first
- * call on a device looks up the array's device address; make that first call before
- * any stream capture. All calls share the array: calls that overlap on the GPU race,
- * so serialise them (one stream, one thread at a time).
+ * rejected with TB_ERR_INVALID_ARGUMENT (e.g. CKKS N=16384 fits up to L=8). The
+ * array's device address is looked up by tb_context_create (which, under lazy module
+ * loading, is when the device takes the 16 MiB), so no call of this function loads
+ * or allocates anything. All calls share the array: calls that overlap on the GPU
+ * race, so serialise them (one stream, one thread at a time).
  */
 int tb_relinearize_noalloc(tb_context *ctx, int L, uint64_t *ct, uint64_t ct_stride, const uint64_t *key,
                            uint64_t batch, void *stream);

@@ -74,6 +74,7 @@ static bool build_ntt_tables(uint64_t q, int logn, std::vector<ulonglong2> &fwd,
 }
 
 int build_rns_levels(Context &c);  // rns.cu
+int noalloc_scratch_address(uint64_t **out);  // keyswitch.cu
 
 int context_create(int scheme, uint64_t n, const uint64_t *moduli, int count, uint64_t t, Context **out) {
     using namespace host;
@@ -140,6 +141,7 @@ int context_create(int scheme, uint64_t n, const uint64_t *moduli, int count, ui
         return status_from(e);
     }
     int st = build_rns_levels(*c);
+    if (st == TB_OK) st = noalloc_scratch_address(&c->noalloc_scratch);
     if (st != TB_OK) {
         delete c;
         return st;

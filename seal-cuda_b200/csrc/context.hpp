@@ -108,6 +108,7 @@ struct Context {
     std::unordered_map<uint32_t, uint32_t *> galois_ntt;
     uint32_t *d_slot_map = nullptr;   // batch-encoder slot -> coefficient map
     void *d_fft_roots = nullptr;      // CKKS special-FFT roots: [N] forward, [N] inverse (double2)
+    uint64_t *noalloc_scratch = nullptr;  // device address of the static relinearize scratch on `device`
     ~Context();
 };
 

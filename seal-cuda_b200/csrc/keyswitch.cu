@@ -618,20 +618,16 @@ constexpr size_t TB_NOALLOC_SCRATCH_BYTES = 16ull << 20;  // 16 MiB: one L=8, N=
 static __device__ __align__(256) uint64_t g_noalloc_scratch[TB_NOALLOC_SCRATCH_BYTES / 8];
 
 // Device address of g_noalloc_scratch on the current device. In host code the
-// array's name only stands in for the symbol, so its address is asked for once per
-// device, with that device current, and cached.
-static int noalloc_scratch(int device, uint64_t **out) {
-    static std::mutex mu;
-    static uint64_t *addr[64] = {nullptr};
-    if (device < 0 || device >= 64) return set_error(TB_ERR_UNSUPPORTED, "device index out of range");
-    std::lock_guard<std::mutex> g(mu);
-    if (!addr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return status_from(e);
-        addr[device] = (uint64_t *)p;
-    }
-    *out = addr[device];
+// array's name only stands in for the symbol, so the address is asked for while a
+// context is created (its device current) and kept in the context. With lazy module
+// loading this lookup is what loads the library's device image, array included, on
+// that device: the 16 MiB are taken at context creation, never inside a relinearize
+// call, and a context created after a device reset gets the new address.
+int noalloc_scratch_address(uint64_t **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return status_from(e);
+    *out = (uint64_t *)p;
     return TB_OK;
 }
 
@@ -654,9 +650,8 @@ int relinearize_noalloc(const Context &c, int L, uint64_t *ct3, uint64_t cstride
                          "relinearize without allocation needs " + std::to_string(per_ct) +
                              " bytes of scratch for one ciphertext at this level; the static scratch holds " +
                              std::to_string(TB_NOALLOC_SCRATCH_BYTES) + " bytes");
-    uint64_t *base = nullptr;
-    int st = noalloc_scratch(c.device, &base);
-    if (st != TB_OK) return st;
+    uint64_t *base = c.noalloc_scratch;
+    if (!base) return set_error(TB_ERR_CUDA, "static relinearize scratch not found on this device");
     const uint64_t chunk = std::min<uint64_t>(B, TB_NOALLOC_SCRATCH_BYTES / per_ct);
     uint64_t *tgt = base;
     uint64_t *digits = tgt + (ckks ? chunk * L * n : 0);

@@ -38,8 +38,12 @@ std::vector<uint64_t> get_words(std::istream &s, std::size_t count) {
     return w;
 }
 
-// Payload limit of one loaded object (a corrupt length must not allocate without bound).
-constexpr std::size_t MAX_WORDS = std::size_t(1) << 34;
+// Largest degree and limb count a context describes: no valid object holds more words
+// per polynomial than their product, so a corrupt length is refused before allocating.
+constexpr std::size_t MAX_DEGREE = std::size_t(1) << 17;
+constexpr std::size_t MAX_LIMBS = 64;
+// Payload limit of a plaintext: one NTT-form polynomial over every limb at the largest degree.
+constexpr std::size_t MAX_WORDS = MAX_DEGREE * MAX_LIMBS;
 
 // A size-2 NTT-form ciphertext header and payload (scale 1, correction 1, no seed):
 // how public keys and every digit of a key-switching key travel.
@@ -102,7 +106,8 @@ void Ciphertext::loadHeader(std::istream &s, bool &terms, std::uint64_t &seed) {
     corr_ = get<std::uint64_t>(s);
     seed = get<std::uint64_t>(s);
     terms = get<bool>(s);
-    if (size_ > 64 || n_ > (std::size_t(1) << 20) || limbs_ > 64) throw std::invalid_argument("ciphertext too large");
+    if (size_ > 64 || n_ > MAX_DEGREE || (n_ & (n_ - 1)) || limbs_ > MAX_LIMBS)
+        throw std::invalid_argument("ciphertext header out of range");
 }
 
 void Ciphertext::load(std::istream &s) {

@@ -59,16 +59,19 @@ def test_sub_batches_keep_every_pairs_rotation_step():
     per rotation step, the sub-batches' runs count exactly the pairs that take it, and
     each sub-batch's runs tile its pairs."""
     import bench
+    import ckks_step
     steps, pairs = len(bench.STEPS_K), bench.DEFAULT_PAIRS
-    whole = {g: cnt for g, _, cnt in bench.rotation_runs(0, pairs, steps)}
+    whole = {g: cnt for g, _, cnt in ckks_step.rotation_runs(0, pairs, steps)}
     assert sum(whole.values()) == pairs
     for count in (1, 2, 4, 8):
         pc = pairs // count
         got = {}
         for c in range(count):
-            runs = bench.rotation_runs(c * pc, pc, steps)
+            runs = ckks_step.rotation_runs(c * pc, pc, steps)
             assert [r[1] for r in runs] == [sum(r[2] for r in runs[:k]) for k in range(len(runs))]
             assert sum(r[2] for r in runs) == pc
             for g, _, cnt in runs:
                 got[g] = got.get(g, 0) + cnt
         assert got == whole
+        rows = ckks_step.row_groups(pairs, count, steps)
+        assert len(rows) == pairs and {g: rows.count(g) for g in set(rows)} == whole

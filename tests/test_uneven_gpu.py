@@ -30,9 +30,9 @@ def test_uneven_batch_graph_streams_per_op_and_reference_agree():
     orc = Oracle("orc")
     t = orc.plain_modulus_batching(16384, 20)
     rng = np.random.default_rng(404)
-    # 96 ciphertexts with degrees drawn uniformly; the first two of each group are real
-    # encryptions made by the reference, the rest uniform residues
-    draws = rng.integers(0, len(SHAPES), 96)
+    # the benchmark's 512 ciphertexts with degrees drawn uniformly; the first two of each
+    # group are real encryptions made by the reference, the rest uniform residues
+    draws = rng.integers(0, len(SHAPES), 512)
     groups, checks = [], []
     for gi, (scheme, n, bits) in enumerate(SHAPES):
         moduli = orc.coeff_modulus_create(n, bits)
