@@ -630,12 +630,15 @@ def roofline(res, steps):
     alg = algorithmic_bytes_per_step(res["L"])
     peak, kind = _peak_hbm()
     table = {}
+    traffic = measured_traffic()
     for name, (launches, total_ms) in trace.items():
         per_launch_ms = total_ms / launches
         b = alg.get(name)
         gbs = (b * steps / launches) / (per_launch_ms * 1e-3) / 1e9 if b else None
         table[name] = {"launches_per_step": launches // steps, "ms_per_step": round(total_ms / steps, 4),
-                       "GBps": round(gbs, 1) if gbs else None}
+                       "GBps": round(gbs, 1) if gbs else None, "frac_hbm": round(gbs / peak, 4) if gbs else None}
+        if name in traffic:
+            table[name]["traffic_per_launch"] = round(traffic[name] * steps / launches)
     name = max(trace.items(), key=lambda kv: kv[1][1])[0]
     launches, total_ms = trace[name]
     per_launch_ms = total_ms / launches

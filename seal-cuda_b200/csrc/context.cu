@@ -269,7 +269,7 @@ static int ntt_plain(const Context &c, const uint64_t *in, uint64_t *out, uint64
     // limbs up to 2^14 in one launch, and 2^15 inverse transforms on two-CTA clusters;
     // longer limbs (and 2^15 forward transforms, measured faster so) split into global
     // top stages and 2^14 sub-blocks
-    const int logb = (logn <= MAX_LOGB || (!FWD && logn == MAX_FUSED_LOGN)) ? logn : MAX_LOGB;
+    const int logb = (logn <= MAX_LOGB || (!FWD && logn == PAIR_LOGN)) ? logn : MAX_LOGB;
     const int h = logn - logb;
     if ((total << h) > 0x7fffffffULL || (h > 0 && total > 65535))
         return set_error(TB_ERR_INVALID_ARGUMENT, "too many limbs in one launch");

@@ -101,6 +101,10 @@ struct StridedNttOp {
 };
 
 // Step 2: forward NTT of digit j (coefficient form) reduced into key modulus i.
+// Only exact residues matter downstream (the inner product reduces its 128-bit sums),
+// so the load leaves its Barrett remainder in [0, 2q) (the transform takes inputs
+// below 4q) and, while the sums stay below 2^128, the store keeps the transform's lazy
+// [0, 4q) outputs: products below 4q * q < 2^124 (q < 2^61), at most 15 of them.
 struct ModUpOp {
     const uint64_t *src;      // CKKS: inverse-transformed targets [B][L][N]; else targets
     uint64_t sstride;         // words between ciphertexts in src
@@ -108,6 +112,7 @@ struct ModUpOp {
     const Mod *mods;
     const uint64_t *chain;    // device copy of chain values (for the reduce test)
     int L, K, ckks, logn;
+    static constexpr int LAZY_MAX_L = 15;   // digits summed lazily from [0, 4q)
     struct Ctx {
         NttLimb lm;
         const uint64_t *in;
@@ -140,12 +145,14 @@ struct ModUpOp {
     __device__ uint64_t load(const Ctx &c, int e) const {
         const uint64_t x = c.in[e];
         if (!c.reduce) return x;
-        const uint64_t q = c.lm.q;
-        const uint64_t r = x - mulhi(x, c.ratio_hi) * q;
-        return r >= q ? r - q : r;
+        return x - mulhi(x, c.ratio_hi) * c.lm.q;   // in [0, 2q)
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
-        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(full_fwd(a, c.lm.q), full_fwd(b, c.lm.q));
+        if (L > LAZY_MAX_L) {
+            a = full_fwd(a, c.lm.q);
+            b = full_fwd(b, c.lm.q);
+        }
+        *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(a, b);
     }
 };
 
@@ -249,19 +256,23 @@ struct ModDownBase {
         c.ct = ct + (size_t)cb * cstride + (((size_t)cc * L + j) << logn);
         return c;
     }
-    __device__ uint64_t last_mod(const Ctx &c, int e) const {
+    // the special-prime residue r mod q_j: in [0, 2q) (lazy), or canonical
+    __device__ uint64_t last_mod_lazy(const Ctx &c, int e) const {
         const uint64_t r = c.last[e];
         if (!c.reduce) return r;
-        const uint64_t q = c.lm.q;
-        const uint64_t x = r - mulhi(r, c.ratio_hi) * q;
-        return x >= q ? x - q : x;
+        return r - mulhi(r, c.ratio_hi) * c.lm.q;
+    }
+    __device__ uint64_t last_mod(const Ctx &c, int e) const {
+        const uint64_t x = last_mod_lazy(c, e);
+        return x >= c.lm.q ? x - c.lm.q : x;
     }
 };
 
 // Step 5, CKKS: NTT of (r mod q_j) + fix, epilogue ct += (acc + 4 q_j - ntt) * q_k^-1.
+// The transform's input only has to stay below 4 q_j: a lazy residue (< 2 q_j) plus fix.
 struct ModDownCkksOp : ModDownBase {
     __device__ Ctx ctx(int b) const { return make(b); }
-    __device__ uint64_t load(const Ctx &c, int e) const { return last_mod(c, e) + c.d.fix; }
+    __device__ uint64_t load(const Ctx &c, int e) const { return last_mod_lazy(c, e) + c.d.fix; }
     // epilogue reads of a coefficient pair: the accumulator and the ciphertext limb
     struct Epi {
         ulonglong2 acc, ct;
@@ -339,7 +350,7 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
     if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
     if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
-    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 32768");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 131072");
     if (!target || !ct || keys.count < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     for (int g = 0; g < keys.count; g++)
         if (!keys.key[g]) return set_error(TB_ERR_NO_KEY, "missing key-switching key");
@@ -637,7 +648,7 @@ int relinearize_noalloc(const Context &c, int L, uint64_t *ct3, uint64_t cstride
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
     if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
     if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
-    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 32768");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused key switching supports N <= 131072");
     if (!ct3 || !key) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     if (B == 0) return TB_OK;
     const uint64_t n = c.n;

@@ -175,18 +175,19 @@ int build_level_consts(Context &c, int L) {
 
 namespace {
 
-constexpr int MAXL = 32;   // data limbs handled by the per-coefficient BEHZ kernels
-constexpr int MAXB = MAXL + 2;
+constexpr int MAXL_RT = 32;  // data limbs of the run-time form (LT = 0)
+constexpr int MAXL = 64;     // data limbs of the wide run-time form (LT = -1): every chain a context takes
 
 __device__ __forceinline__ uint64_t pw(const uint64_t *K, int off, int i, uint64_t x, uint64_t q) {
     return mul_shoup(x, K[off + 2 * i], K[off + 2 * i + 1], q);
 }
 
 // The per-coefficient BEHZ kernels are templates over the data-limb count LT, with LT = 0
-// the run-time form for any count up to MAXL. With LT fixed the loops over the data limbs
-// unroll and the per-coefficient residues and accumulators stay in registers; the loops
-// over the B / Bsk primes stay rolled, so one iteration's constants are all that is live
-// beside them.
+// the run-time form for any count up to MAXL_RT and LT = -1 the same form with arrays for
+// MAXL limbs (its per-coefficient arrays live in local memory). With LT fixed the loops
+// over the data limbs unroll and the per-coefficient residues and accumulators stay in
+// registers; the loops over the B / Bsk primes stay rolled, so one iteration's constants
+// are all that is live beside them.
 
 // Steps (1)+(2): q (coefficient form) -> Bsk, one coefficient per thread, for both
 // inputs of B products: polynomial p = ct*4 + slot, slots 0,1 from a and 2,3 from b;
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(256, 3) behz_lift_kernel(const uint64_t *__res
                                                         uint64_t *__restrict__ dst, const Mod *__restrict__ qm,
                                                         const Mod *__restrict__ bm, const uint64_t *__restrict__ K,
                                                         RnsOff o, int L_, int bsk, int logn, uint64_t P) {
-    constexpr int NL = LT > 0 ? LT : MAXL, UNROLL = LT > 0 ? LT : 1;
+    constexpr int NL = LT > 0 ? LT : (LT == 0 ? MAXL_RT : MAXL), UNROLL = LT > 0 ? LT : 1;
     const int L = LT > 0 ? LT : L_;
     const uint32_t n = 1u << logn;
     const uint64_t total = P << logn;
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256, 2) behz_floor_sk_kernel(const uint64_t *_
                                                             const Mod *__restrict__ qm, const Mod *__restrict__ bm,
                                                             const uint64_t *__restrict__ K, RnsOff o, int L_, int bB,
                                                             int logn, uint64_t P) {
-    constexpr int NL = LT > 0 ? LT : MAXL, UNROLL = LT > 0 ? LT : 1;
+    constexpr int NL = LT > 0 ? LT : (LT == 0 ? MAXL_RT : MAXL), UNROLL = LT > 0 ? LT : 1;
     const int L = LT > 0 ? LT : L_;
     const int bsk = bB + 1;
     const uint32_t n = 1u << logn;
@@ -324,7 +325,7 @@ struct FloorLaunch {
 };
 
 // Launches a BEHZ kernel with the data-limb count fixed for L <= 16, the run-time form
-// otherwise.
+// up to 32 limbs and its wide form above.
 #define TB_BEHZ_CASE(LV) \
     case LV:             \
         return Launch<LV>::run(threads, s, args...);
@@ -335,7 +336,8 @@ cudaError_t behz_dispatch(int L, uint64_t threads, cudaStream_t s, A... args) {
         TB_BEHZ_CASE(7) TB_BEHZ_CASE(8) TB_BEHZ_CASE(9) TB_BEHZ_CASE(10) TB_BEHZ_CASE(11) TB_BEHZ_CASE(12)
         TB_BEHZ_CASE(13) TB_BEHZ_CASE(14) TB_BEHZ_CASE(15) TB_BEHZ_CASE(16)
     default:
-        return Launch<0>::run(threads, s, args...);
+        if (L <= MAXL_RT) return Launch<0>::run(threads, s, args...);
+        return Launch<-1>::run(threads, s, args...);
     }
 }
 #undef TB_BEHZ_CASE
@@ -455,7 +457,7 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     if (!ostride) ostride = 3ull * L * n;
     if (c.scheme == SCHEME_CKKS) return tensor_product_mods(c, c.d_mods, L, a, astride, b, bstride, out, ostride, B, s);
     if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV) return set_error(TB_ERR_UNSUPPORTED, "scheme has no multiply");
-    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 32768");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 131072");
     ensure_pool_retains(c.device);
     const int logn = c.logn;
     cudaError_t e;
@@ -481,7 +483,7 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     // BFV
     const RnsLevel &lv = c.levels[L];
     if (!lv.d_consts) return set_error(TB_ERR_UNSUPPORTED, "plain modulus not coprime to the coefficient moduli");
-    if (L > MAXL) return set_error(TB_ERR_UNSUPPORTED, "BFV multiply supports at most 32 data limbs");
+    if (L > MAXL) return set_error(TB_ERR_UNSUPPORTED, "BFV multiply supports at most 64 data limbs");
     const int bsk = lv.bsk;
     const uint64_t pq = (uint64_t)L * n, pb = (uint64_t)bsk * n;
     ScratchBuf buf(s);
@@ -564,7 +566,7 @@ int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uin
     if (sa < 2 || sb < 2 || sa > 64 || sb > 64) return set_error(TB_ERR_INVALID_ARGUMENT, "ciphertext sizes must be 2 .. 64");
     if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV && c.scheme != SCHEME_CKKS)
         return set_error(TB_ERR_UNSUPPORTED, "scheme has no multiply");
-    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 32768");
+    if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 131072");
     const int logn = c.logn;
     const uint64_t n = c.n, pq = (uint64_t)L * n;
     const int P = sa + sb, D = sa + sb - 1;
@@ -597,7 +599,7 @@ int multiply_sizes(const Context &c, int L, const uint64_t *a, int sa, const uin
     // BFV
     const RnsLevel &lv = c.levels[L];
     if (!lv.d_consts) return set_error(TB_ERR_UNSUPPORTED, "plain modulus not coprime to the coefficient moduli");
-    if (L > MAXL) return set_error(TB_ERR_UNSUPPORTED, "BFV multiply supports at most 32 data limbs");
+    if (L > MAXL) return set_error(TB_ERR_UNSUPPORTED, "BFV multiply supports at most 64 data limbs");
     const int bsk = lv.bsk;
     const uint64_t pb = (uint64_t)bsk * n;
     e = cudaMallocAsync(&buf.p, ((uint64_t)P * (2 * pq + pb) + (uint64_t)D * (pq + pb)) * 8, s);

@@ -384,6 +384,135 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THR
     for (int e = threadIdx.x; e < NB; e += T) op.store(c, e + off, sm[swz(e)]);
 }
 
+// ---------------------------------------------------------------- clusters of 4 and 8 CTAs
+// A limb of 2^(LOGB+CLOG) coefficients (CLOG = 2, 3: N = 65536, 131072 at LOGB = 14)
+// transformed by a cluster of 2^CLOG CTAs, CTA r holding block r (coefficients
+// r 2^LOGB .. (r+1) 2^LOGB - 1) in its shared memory. The stages whose butterflies join
+// two blocks (forward: the first CLOG; inverse: the last CLOG, the N^-1-scaled one last)
+// run between cluster barriers: the two CTAs of a pair of partner blocks each compute
+// half of the pair's butterflies, reading and writing both blocks through distributed
+// shared memory. Every other stage runs inside a block exactly as the sub-block passes
+// of the split transform. The butterflies and their order are those of the split
+// transform, so outputs (lazy values included) are the same, and the Op's loads and
+// stores see whole-limb coefficient indices as in every other form.
+
+// One cross-block stage over partner blocks xs (lower) and ys (upper): this CTA takes
+// butterflies j0 .. j0 + NB/2 - 1 of the pair (the same slot in both blocks).
+template <bool FWD, bool SCALE, int NB, int T>
+__device__ __forceinline__ void cross_stage(uint64_t *xs, uint64_t *ys, int j0, ulonglong2 w, const NttLimb &lm) {
+    constexpr int IT = NB / 2 / T;
+    constexpr int U = IT >= 4 ? 4 : IT;
+    static_assert(IT * T == NB / 2 && IT % U == 0, "cross stage split");
+    const uint64_t q = lm.q, q2 = q << 1;
+#pragma unroll 1
+    for (int i0 = 0; i0 < IT; i0 += U) {
+        uint64_t x[U], y[U];
+        int p[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            p[u] = swz(j0 + threadIdx.x + (i0 + u) * T);
+            x[u] = xs[p[u]];
+            y[u] = ys[p[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if constexpr (FWD) {
+                ct_butterfly(x[u], y[u], w, q, q2);
+            } else if constexpr (SCALE) {
+                const uint64_t a = x[u] >= q2 ? x[u] - q2 : x[u];
+                uint64_t sum = a + y[u];
+                sum = sum >= q2 ? sum - q2 : sum;
+                const uint64_t dif = a + q2 - y[u];
+                x[u] = mul_shoup_lazy(sum, lm.inv_n, lm.inv_n_quo, q);
+                y[u] = mul_shoup_lazy(dif, lm.sroot, lm.sroot_quo, q);
+            } else {
+                gs_butterfly(x[u], y[u], w, q, q2);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            xs[p[u]] = x[u];
+            ys[p[u]] = y[u];
+        }
+    }
+}
+
+template <int LOGB, int CLOG, class Op>
+__global__ void __cluster_dims__(1 << CLOG, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+    ntt_fwd_cluster_kernel(Op op) {
+    namespace cg = cooperative_groups;
+    extern __shared__ uint64_t sm[];
+    constexpr int NB = 1 << LOGB, C = 1 << CLOG;
+    constexpr int T = NttCfg<LOGB, 0>::THREADS;
+    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned r = cl.block_rank();
+    auto c = op.ctx((int)(blockIdx.x >> CLOG));
+    c.lm.sb = r;
+    const int off = (int)r << LOGB;
+    for (int j = threadIdx.x; j < NB; j += T) sm[swz(j)] = op.load(c, j + off);
+    cl.sync();   // every block loaded (and every input read: in-place stores are safe later)
+#pragma unroll
+    for (int s = 0; s < CLOG; s++) {
+        const unsigned G = (unsigned)C >> (s + 1);   // partner distance in blocks
+        const unsigned lo = r & ~G;
+        const ulonglong2 w = __ldg(c.lm.roots + (1u << s) + (lo >> (CLOG - s)));
+        cross_stage<true, false, NB, T>(cl.map_shared_rank(sm, lo), cl.map_shared_rank(sm, lo | G),
+                                        (r & G) ? NB / 2 : 0, w, c.lm);
+        cl.sync();
+    }
+    const uint32_t rbase = (1u << CLOG) + r;   // global stage CLOG onwards, sub-block = r
+    constexpr int FIRST = REM != 0 ? REM : 3;
+    fwd_pass<FIRST, false, LOGB, T, 0, false>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
+    fwd_copy_out<NB, T>(op, c, sm, off);
+}
+
+template <int LOGB, int CLOG, class Op>
+__global__ void __cluster_dims__(1 << CLOG, 1, 1) __launch_bounds__(NttCfg<LOGB, 0>::THREADS)
+    ntt_inv_cluster_kernel(Op op) {
+    namespace cg = cooperative_groups;
+    extern __shared__ uint64_t sm[];
+    constexpr int NB = 1 << LOGB;
+    constexpr int LOGN = LOGB + CLOG;
+    constexpr uint32_t N = 1u << LOGN;
+    constexpr int T = NttCfg<LOGB, 0>::THREADS;
+    constexpr int REM = NttCfg<LOGB, 0>::REM;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned r = cl.block_rank();
+    auto c = op.ctx((int)(blockIdx.x >> CLOG));
+    c.lm.sb = r;
+    const int off = (int)r << LOGB;
+    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
+        uint64_t a, b;
+        op.load2(c, e + off, a, b);
+        const int p = swz(e);
+        *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
+    }
+    __syncthreads();
+    constexpr int LAST = REM ? REM : 3;
+    constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;
+    inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, LOGN);
+    inv_pass<LAST, false, false, LOGB, T, 3 * PASSES, false>(op, c, sm, LOGN);
+    cl.sync();
+#pragma unroll
+    for (int s = 0; s < CLOG; s++) {
+        const unsigned G = 1u << s;   // global stage LOGB + s joins blocks G apart
+        const unsigned lo = r & ~G;
+        uint64_t *xs = cl.map_shared_rank(sm, lo), *ys = cl.map_shared_rank(sm, lo | G);
+        const int j0 = (r & G) ? NB / 2 : 0;
+        if (s + 1 < CLOG) {
+            const int sg = LOGB + s;
+            const ulonglong2 w = __ldg(c.lm.iroots + (N + 1 - (N >> sg) + (lo >> (s + 1))));
+            cross_stage<false, false, NB, T>(xs, ys, j0, w, c.lm);
+        } else {
+            cross_stage<false, true, NB, T>(xs, ys, j0, make_ulonglong2(0, 0), c.lm);
+        }
+        cl.sync();
+    }
+    for (int e = threadIdx.x; e < NB; e += T) op.store(c, e + off, sm[swz(e)]);
+}
+
 template <int LOGB>
 inline size_t ntt_smem_bytes() {
     return sizeof(uint64_t) * (size_t)(1 << LOGB);
@@ -403,7 +532,9 @@ __device__ __forceinline__ NttLimb make_limb(const Mod &m, uint32_t sb) {
 }
 
 constexpr int MAX_LOGB = 14;  // 16384 coefficients = 128 KB of shared memory per CTA
-constexpr int MAX_FUSED_LOGN = MAX_LOGB + 1;  // longest limb of the fused operations (a CTA pair)
+constexpr int PAIR_LOGN = MAX_LOGB + 1;   // whole limbs on a CTA pair
+constexpr int MAX_CLUSTER_LOG = 3;        // clusters of up to 8 CTAs (the portable size)
+constexpr int MAX_FUSED_LOGN = MAX_LOGB + MAX_CLUSTER_LOG;  // longest limb of the fused operations
 
 template <int LOGB, int V, class Op>
 inline cudaError_t launch_fwd(const Op &op, unsigned blocks, int s0, cudaStream_t s) {
@@ -455,6 +586,43 @@ inline cudaError_t launch_pair(const Op &op, unsigned blocks, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Whole limbs of 2^(LOGB+CLOG) coefficients, one cluster of 2^CLOG CTAs each (forward
+// from stage 0, inverse with the N^-1 scaling). A device that cannot hold one such
+// cluster at once is refused before the launch.
+template <bool FWD, int LOGB, int CLOG, class Op>
+inline cudaError_t launch_cluster(const Op &op, unsigned blocks, cudaStream_t s) {
+    if (blocks > (0x7fffffffu >> CLOG)) return cudaErrorInvalidValue;
+    const size_t smem = ntt_smem_bytes<LOGB>();
+    constexpr int T = NttCfg<LOGB, 0>::THREADS;
+    auto k = [] {
+        if constexpr (FWD) return ntt_fwd_cluster_kernel<LOGB, CLOG, Op>;
+        else return ntt_inv_cluster_kernel<LOGB, CLOG, Op>;
+    }();
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    static int fits = -1;   // per instantiation: clusters that can be resident at once
+    if (fits < 0) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = 1u << CLOG;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(1u << CLOG);
+        cfg.blockDim = dim3(T);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        e = cudaOccupancyMaxActiveClusters(&n, k, &cfg);
+        if (e != cudaSuccess) return e;
+        fits = n;
+    }
+    if (fits < 1) return cudaErrorInvalidClusterSize;
+    k<<<blocks << CLOG, T, smem, s>>>(op);
+    return cudaGetLastError();
+}
+
 template <bool FWD, int LOGB, int V, class Op>
 inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
     if constexpr (V >= 3) {
@@ -479,8 +647,9 @@ inline int small_launch_variant(int v, unsigned blocks) {
 }
 
 // Dispatch on log2 of the CTA block (1 .. 14); block sizes 2^12 .. 2^14 carry variants
-// with half and a quarter of the threads and their CTA-pair forms. 15: whole 2^15 limbs
-// on CTA pairs (forward from stage 0 only, inverse with the scaling only).
+// with half and a quarter of the threads and their CTA-pair forms. 15, 16, 17: whole
+// limbs of 2^15, 2^16, 2^17 coefficients on CTA pairs and clusters of 4 and 8 CTAs
+// (forward from stage 0 only, inverse with the scaling only).
 template <bool FWD, class Op>
 cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn, int scale_last, cudaStream_t s) {
 #define TB_CASE(B) \
@@ -505,9 +674,15 @@ cudaError_t dispatch_ntt(int logb, const Op &op, unsigned blocks, int s0_or_logn
     switch (logb) {
         TB_CASE(1) TB_CASE(2) TB_CASE(3) TB_CASE(4) TB_CASE(5) TB_CASE(6) TB_CASE(7)
         TB_CASE(8) TB_CASE(9) TB_CASE(10) TB_CASE(11) TB_CASE2(12) TB_CASE2(13) TB_CASE2(14)
-    case MAX_FUSED_LOGN:
-        if (FWD ? s0_or_logn != 0 : (s0_or_logn != MAX_FUSED_LOGN || !scale_last)) return cudaErrorInvalidValue;
+    case PAIR_LOGN:
+        if (FWD ? s0_or_logn != 0 : (s0_or_logn != PAIR_LOGN || !scale_last)) return cudaErrorInvalidValue;
         return launch_pair<FWD, MAX_LOGB, 0>(op, blocks, s);
+    case MAX_LOGB + 2:
+        if (FWD ? s0_or_logn != 0 : (s0_or_logn != MAX_LOGB + 2 || !scale_last)) return cudaErrorInvalidValue;
+        return launch_cluster<FWD, MAX_LOGB, 2>(op, blocks, s);
+    case MAX_LOGB + 3:
+        if (FWD ? s0_or_logn != 0 : (s0_or_logn != MAX_LOGB + 3 || !scale_last)) return cudaErrorInvalidValue;
+        return launch_cluster<FWD, MAX_LOGB, 3>(op, blocks, s);
     default:
         return cudaErrorInvalidValue;
     }

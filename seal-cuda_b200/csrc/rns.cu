@@ -121,13 +121,10 @@ struct RescaleNttOp {
         c.r = r + ((size_t)p << logn);
         return c;
     }
+    // the transform takes any input below 4 q_j: the Barrett remainder (< 2 q_j) plus fix
     __device__ uint64_t load(const Ctx &c, int e) const {
         uint64_t x = c.r[e];
-        if (c.reduce) {
-            const uint64_t q = c.lm.q;
-            x = x - mulhi(x, c.ratio_hi) * q;
-            x = x >= q ? x - q : x;
-        }
+        if (c.reduce) x = x - mulhi(x, c.ratio_hi) * c.lm.q;
         return x + c.d.fix;
     }
     // epilogue reads of a coefficient pair: the limb being rescaled
@@ -213,7 +210,7 @@ int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, 
     const uint64_t P = B * size;
     cudaError_t e;
     if (c.scheme == SCHEME_CKKS) {
-        if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused rescale supports N <= 32768");
+        if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "fused rescale supports N <= 131072");
         ensure_pool_retains(c.device);
         uint64_t *r = nullptr;
         e = cudaMallocAsync(&r, P * n * 8, s);

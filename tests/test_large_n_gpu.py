@@ -1,6 +1,10 @@
-"""Ring degree 32768 through the fused operations (each limb on a two-CTA cluster):
-seeded BFV, BGV and CKKS chains (encrypt, multiply, relinearize, rotate, mod-switch /
-rescale) give the reference CPU path's words at every step."""
+"""Ring degrees 32768, 65536 and 131072 through the fused operations (each limb on a
+cluster of two, four or eight CTAs exchanging the stages that join their blocks
+through distributed shared memory): seeded BFV, BGV and CKKS chains (encrypt,
+multiply, relinearize, rotate, mod-switch / rescale) give the reference CPU path's
+words at every step. Degrees above 32768 have no 128-bit security table in the
+reference, so every context here is made with SecurityLevel.none, as the reference
+session is."""
 import numpy as np
 import pytest
 
@@ -9,7 +13,8 @@ torch = pytest.importorskip("torch")
 pytroy = pytest.importorskip("pytroy")
 from oracle import RefSession, available  # noqa: E402
 
-N = 32768
+N = 32768   # the BFV test with more than 16 data limbs
+DEGREES = [32768, 65536, 131072]
 SEED = [int(x) for x in range(101, 109)]
 S = pytroy.SchemeType
 
@@ -22,22 +27,23 @@ def _same(ref, rid, ct):
     return np.array_equal(ref.ct(rid)["data"].reshape(-1), _words(ct))
 
 
-def _context(scheme, bits, t=None):
+def _context(scheme, bits, t=None, n=N):
     p = pytroy.EncryptionParameters(scheme)
-    p.set_poly_modulus_degree(N)
-    p.set_coeff_modulus(pytroy.CoeffModulus.create(N, bits))
+    p.set_poly_modulus_degree(n)
+    p.set_coeff_modulus(pytroy.CoeffModulus.create(n, bits))
     if t is not None:
         p.set_plain_modulus(t)
     p.set_random_generator(pytroy.Blake2xbPRNGFactory(SEED))
-    return pytroy.SEALContext(p)
+    return pytroy.SEALContext(p, True, pytroy.SecurityLevel.none)
 
 
 @pytest.mark.skipif(not available("ref"), reason="reference library not built")
+@pytest.mark.parametrize("N", DEGREES)
 @pytest.mark.parametrize("scheme", [S.bfv, S.bgv], ids=["bfv", "bgv"])
-def test_batched_schemes_at_32768_match_reference_words(scheme):
+def test_batched_schemes_at_large_degrees_match_reference_words(scheme, N):
     bits = [50, 50, 50, 50, 60]
     t = pytroy.PlainModulus.batching(N, 20)
-    ctx = _context(scheme, bits, t)
+    ctx = _context(scheme, bits, t, N)
     moduli = [m.value() for m in pytroy.CoeffModulus.create(N, bits)]
     ref = RefSession(int(scheme.value), N, moduli, t.value(), np.array(SEED, np.uint64))
     keygen = pytroy.KeyGenerator(ctx)
@@ -72,10 +78,11 @@ def test_batched_schemes_at_32768_match_reference_words(scheme):
 
 
 @pytest.mark.skipif(not available("ref"), reason="reference library not built")
-def test_ckks_at_32768_matches_reference_words():
+@pytest.mark.parametrize("N", DEGREES)
+def test_ckks_at_large_degrees_matches_reference_words(N):
     bits = [60, 40, 40, 40, 60]
     scale = 2.0 ** 40
-    ctx = _context(S.ckks, bits)
+    ctx = _context(S.ckks, bits, None, N)
     moduli = [m.value() for m in pytroy.CoeffModulus.create(N, bits)]
     ref = RefSession(2, N, moduli, 0, np.array(SEED, np.uint64))
     keygen = pytroy.KeyGenerator(ctx)

@@ -32,6 +32,7 @@ def _rand(rng, moduli, n, lead):
     (8192, [43, 43, 44, 44, 44], None),
     (16384, [48] * 9, None),
     (64, [40, 40, 40, 40], None),
+    (4096, [50] * 41, 65537),   # 40 and 41 data limbs: the wide run-time form
 ])
 def test_bfv_multiply(orc, n, bits, t):
     moduli = orc.coeff_modulus_create(n, bits)
