@@ -15,7 +15,9 @@ prime (the arithmetic performed is the same as on encrypted data).
 
 * ``value``: ops/s with inputs resident in HBM (CUDA events on the launch stream,
   max over ranks). Inputs (2 x 128 MB) exceed the 126 MB L2 between steps. Each
-  step's 64 pairs run as S concurrent sub-batches, one stream each (default 4).
+  step's 64 pairs run as S concurrent sub-batches, one stream each (default 4), the
+  whole fork/join captured once as a CUDA graph and replayed per step (--no-graph:
+  eager launches).
 * ``e2e``: the same metric through the C ABI with host buffers: every step copies
   both operand batches from pinned host memory and reads the results back, as 4
   sub-batches whose copies run on one stream per direction, overlapping the
@@ -222,15 +224,33 @@ def run_b200(args, rank, world):
     for _ in range(args.warmup):
         step(A, B, O)
     barrier()
+    graph = None
+    if args.graph:
+        # the whole step (sub-batches, fork and join) captured once as a CUDA graph: the
+        # library builds its per-element tables during the warm-up steps, and its
+        # stream-ordered scratch allocations become graph memory nodes
+        graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream()
+        cap.wait_stream(stream)
+        with torch.cuda.graph(graph, stream=cap, capture_error_mode="relaxed"):
+            step(A, B, O, st=cap)
+        stream.wait_stream(cap)
+        for _ in range(args.warmup):
+            graph.replay()
+        barrier()
     clocks = ClockSampler(dev)
     clocks.start()
-    lib.tb_trace_enable(1)
+    if not graph:
+        lib.tb_trace_enable(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")
     clocks.mark()
     e0.record(stream)
     for _ in range(args.steps):
-        step(A, B, O)
+        if graph:
+            graph.replay()
+        else:
+            step(A, B, O)
     e1.record(stream)
     torch.cuda.nvtx.range_pop()
     barrier()
@@ -238,11 +258,22 @@ def run_b200(args, rank, world):
     clk = clocks.stop()
     entries = (tb_capi_trace_entry * 64)()
     cnt = ctypes.c_int()
-    tb_capi.check(lib.tb_trace_collect(entries, 64, ctypes.byref(cnt)))
-    lib.tb_trace_enable(0)
-    trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms)) for i in range(cnt.value)}
-    launches = sum(v[0] for v in trace.values()) // args.steps
-    if SUB > 1:
+    if graph:
+        # the graph replays the launches of one eager step: count them on one, traced
+        lib.tb_trace_enable(1)
+        step(A, B, O)
+        barrier()
+        tb_capi.check(lib.tb_trace_collect(entries, 64, ctypes.byref(cnt)))
+        lib.tb_trace_enable(0)
+        launches = sum(int(entries[i].launches) for i in range(cnt.value))
+        trace = None
+    else:
+        tb_capi.check(lib.tb_trace_collect(entries, 64, ctypes.byref(cnt)))
+        lib.tb_trace_enable(0)
+        trace = {entries[i].name.decode(): (int(entries[i].launches), float(entries[i].total_ms))
+                 for i in range(cnt.value)}
+        launches = sum(v[0] for v in trace.values()) // args.steps
+    if SUB > 1 or graph:
         # kernels of concurrent sub-batches share the GPU, so their event times say
         # nothing about one kernel: the per-kernel table and the roofline come from the
         # same step as one batch on one stream (kernels alone on the GPU), timed apart
@@ -838,6 +869,8 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference CUDA path")
     ap.add_argument("--streams", type=int, default=HEADLINE_SUB_BATCHES,
                     help="concurrent sub-batches (one stream each) per step of the headline workload")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="time the step as eager launches instead of one captured CUDA graph per step")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch settings (for profiler captures: no tuning launches first)")
     ap.add_argument("--pairs", type=int, default=DEFAULT_PAIRS,
@@ -906,7 +939,7 @@ def main():
                 "config": {"workload": WORKLOAD, "global_batch": ops_total, "seq_len": N,
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "l2": "inputs (256 MB) larger than L2", "tuned": res["tuned"],
-                           "concurrent_sub_batches": res["sub"]},
+                           "concurrent_sub_batches": res["sub"], "cuda_graph": bool(args.graph)},
                 "e2e": {"value": round(e2e, 2), "unit": "ops/s", "h2d_bytes_per_step": res["h2d"],
                         "d2h_bytes_per_step": res["d2h"], "sub_batches_per_step": res["e2e_chunks"]},
                 "gpu_launches": res["launches"],

@@ -112,7 +112,7 @@ int tb_tensor_product(tb_context *ctx, int first, int L, const uint64_t *a, uint
  * fastFloor / fastbconvSk, src/utils/rns_cuda.cu:339-443), BGV by NTT-tensor-INTT
  * (src/evaluator_cuda.cu:435-501), CKKS by the NTT-domain tensor
  * (src/evaluator_cuda.cu:384-432). Strides 0 = packed (2*L*n in, 3*L*n out); out must
- * not overlap the inputs. BFV needs L <= 32.
+ * not overlap the inputs. BFV takes up to 64 data limbs.
  */
 int tb_multiply(tb_context *ctx, int L, const uint64_t *a, uint64_t a_stride, const uint64_t *b, uint64_t b_stride,
                 uint64_t *out, uint64_t out_stride, uint64_t batch, void *stream);
@@ -241,6 +241,19 @@ int tb_encrypt(tb_context *ctx, const uint64_t *seed8, const uint64_t *pk, int L
 int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
                          uint64_t plain_stride, uint64_t plain_count, uint64_t *ct, uint64_t ct_stride,
                          uint64_t batch, void *stream);
+/*
+ * Symmetric encryption in the seed-compressed form of the reference's GPU path
+ * (EncryptorCuda::encryptSymmetric -> util::encryptZeroSymmetric,
+ * src/utils/rlwe_cuda.cu:262-331, saved by CiphertextCuda::save as c0 plus the seed,
+ * src/ciphertext_cuda.cu:8-35): the second polynomial is the cuRAND expansion of a
+ * 64-bit seed (what tb_expand_seeded and the reference's loader regenerate), seeds[b]
+ * (a host array of `batch` words) receives each ciphertext's seed, so only c0 and the
+ * seed need to travel. BFV and CKKS; BGV is refused (the reference's loader leaves a
+ * BGV c1 in the NTT domain). Waits for the seeds to reach the host.
+ */
+int tb_encrypt_symmetric_seeded(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, int L,
+                                const uint64_t *plain, uint64_t plain_stride, uint64_t plain_count, uint64_t *ct,
+                                uint64_t ct_stride, uint64_t *seeds, uint64_t batch, void *stream);
 /*
  * The second polynomial ([L][n]) of a seed-compressed ciphertext, regenerated as the
  * reference's GPU loader does (CiphertextCuda::load with a context,
@@ -399,6 +412,45 @@ int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflie
    value; 0 restores the default). */
 int tb_keyswitch_set_budget(uint64_t bytes);
 uint64_t tb_keyswitch_get_budget(void);
+
+/* ----------------------------------------------------------- uneven batches */
+
+/*
+ * Batches of ciphertexts with different ring degrees and modulus chains: each shape
+ * group is `count` size-2 ciphertext pairs of one context at level L (a, b:
+ * [count][2][L][n] device words), multiplied, relinearized with relin_key and rotated
+ * by galois_elt with galois_key into out ([count][2][L][n]). The reference drives
+ * these operations one ciphertext per call (EvaluatorCuda::multiply /
+ * relinearizeInplace / applyGaloisInplace, src/evaluator_cuda.cu:262-382, 703-744,
+ * 2011-2163); the batch has no counterpart there. The buffers must stay valid for the
+ * batch's lifetime; a captured batch replays on the same buffers.
+ */
+typedef struct {
+    tb_context *ctx;
+    int L;
+    uint64_t count;
+    const uint64_t *a, *b;
+    const uint64_t *relin_key, *galois_key;
+    uint32_t galois_elt;
+    uint64_t *out;
+} tb_uneven_group;
+
+typedef struct tb_uneven tb_uneven;
+
+/* Validates the groups (every context on one device) and allocates the products'
+   scratch, one stream per group and the events of the fork/join. */
+int tb_uneven_create(const tb_uneven_group *groups, int count, tb_uneven **out);
+/* Every group's pipeline as batched calls on a stream of its own, forked from and
+   joined back to `stream` (asynchronous). */
+int tb_uneven_run(tb_uneven *batch, void *stream);
+/* The same pipelines one ciphertext per call on `stream`: the reference's usage. */
+int tb_uneven_run_per_op(tb_uneven *batch, void *stream);
+/* Records tb_uneven_run once as a CUDA graph (after one uncaptured run, so every table
+   and pool setting made on first use exists; waits for it). */
+int tb_uneven_capture(tb_uneven *batch);
+/* One graph launch of the whole captured batch on `stream`. */
+int tb_uneven_replay(tb_uneven *batch, void *stream);
+int tb_uneven_destroy(tb_uneven *batch);
 
 /* ---------------------------------------------------------------- tracing */
 

@@ -143,3 +143,51 @@ extern "C" int ref_gpu_seeded_ct(int scheme, size_t n, const uint64_t *moduli, i
         return 1;
     }
 }
+
+// The reverse direction: wire bytes of a ciphertext made elsewhere (here: this
+// library's seed-compressed symmetric encryption) loaded by the reference GPU path's
+// own loader with a context (CiphertextCuda::load, src/ciphertext_cuda.cu:137-184),
+// decrypted with the secret key of the same seeded factory and decoded: BFV slots
+// into values, CKKS real parts into reals (nvalues of them). words: 2 * L * n, the
+// loaded ciphertext.
+extern "C" int ref_gpu_load_decrypt(int scheme, size_t n, const uint64_t *moduli, int count, uint64_t t,
+                                    const uint64_t *seed8, const char *bytes, size_t len, uint64_t *values,
+                                    double *reals, size_t nvalues, uint64_t *words) {
+    try {
+        KernelProvider::initialize();
+        troy::EncryptionParameters host((SchemeType)scheme);
+        host.setPolyModulusDegree(n);
+        std::vector<Modulus> q;
+        for (int i = 0; i < count; i++) q.emplace_back(moduli[i]);
+        host.setCoeffModulus(q);
+        if ((SchemeType)scheme != SchemeType::ckks) host.setPlainModulus(Modulus(t));
+        troy::PRNGSeed seed;
+        std::copy_n(seed8, 8, seed.begin());
+        host.setRandomGenerator(std::make_shared<troy::Blake2xbPRNGFactory>(seed));
+        EncryptionParameters parms(host);
+        SEALContext context(parms, true, SecurityLevel::none);
+        KeyGenerator keygen(context);
+        Ciphertext c;
+        std::istringstream is(std::string(bytes, len));
+        c.load(is, context);
+        const size_t w = c.size() * c.coeffModulusSize() * c.polyModulusDegree();
+        cudaMemcpy(words, c.data().get(), w * 8, cudaMemcpyDeviceToHost);
+        Decryptor decryptor(context, keygen.secretKey());
+        Plaintext p;
+        decryptor.decrypt(c, p);
+        if ((SchemeType)scheme == SchemeType::ckks) {
+            CKKSEncoder encoder(context);
+            std::vector<std::complex<double>> v;
+            encoder.decode(p, v);
+            for (size_t i = 0; i < nvalues && i < v.size(); i++) reals[i] = v[i].real();
+        } else {
+            BatchEncoder encoder(context);
+            std::vector<uint64_t> v;
+            encoder.decode(p, v);
+            for (size_t i = 0; i < nvalues && i < v.size(); i++) values[i] = v[i];
+        }
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    } catch (...) {
+        return 1;
+    }
+}

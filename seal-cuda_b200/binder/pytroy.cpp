@@ -294,6 +294,7 @@ class ParmsID(list):
                  std::istringstream s{std::string(b)};
                  c.loadTerms(s, ev, from_array(terms));
              })
+        .def("seed", py::overload_cast<>(&Ciphertext::seed, py::const_))
         .def("data", [](const Ciphertext &c) { return to_array(c.toHost()); });
 
     py::class_<KeyGenerator>(m, "KeyGenerator")
@@ -486,9 +487,21 @@ class ParmsID(list):
                  self.encryptZeroSymmetric(r);
                  return r;
              })
-        .def("encrypt_zero_symmetric", [](const Encryptor &self, ParmsID id) {
+        .def("encrypt_zero_symmetric",
+             [](const Encryptor &self, ParmsID id) {
+                 Ciphertext r;
+                 self.encryptZeroSymmetric(id, r);
+                 return r;
+             })
+        .def("encrypt_symmetric_seeded",
+             [](const Encryptor &self, const Plaintext &plain) {
+                 Ciphertext r;
+                 self.encryptSymmetricSeeded(plain, r);
+                 return r;
+             })
+        .def("encrypt_zero_symmetric_seeded", [](const Encryptor &self, ParmsID id) {
             Ciphertext r;
-            self.encryptZeroSymmetric(id, r);
+            self.encryptZeroSymmetricSeeded(id, r);
             return r;
         });
 

@@ -39,7 +39,7 @@ int encrypt(Context &c, const uint64_t *seed8, const uint64_t *pk, int L, const 
             uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t count, cudaStream_t s);
 int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
                       uint64_t pstride, uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t count,
-                      cudaStream_t s);
+                      cudaStream_t s, uint64_t *seeds);
 int decrypt(Context &c, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t cstride, uint64_t *out,
             uint64_t ostride, uint64_t correction, uint64_t B, cudaStream_t s);
 int expand_seeded(Context &c, int L, uint64_t seed, bool inverse_ntt, uint64_t *c1, cudaStream_t s);
@@ -80,9 +80,6 @@ int rescale_to_next(Context &c, int L, const uint64_t *in, uint64_t cstride_in, 
                     int size, uint64_t B, cudaStream_t s);
 }  // namespace tb
 
-struct tb_context {
-    tb::Context *c;
-};
 
 using tb::set_error;
 
@@ -301,7 +298,18 @@ int tb_encrypt_symmetric(tb_context *ctx, const uint64_t *seed8, const uint64_t 
     return on_device(ctx, [&](tb::Context &c) {
         if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
         return tb::encrypt_symmetric(c, seed8, sk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch,
-                                     S(stream));
+                                     S(stream), nullptr);
+    });
+}
+
+int tb_encrypt_symmetric_seeded(tb_context *ctx, const uint64_t *seed8, const uint64_t *sk, int L,
+                                const uint64_t *plain, uint64_t plain_stride, uint64_t plain_count, uint64_t *ct,
+                                uint64_t ct_stride, uint64_t *seeds, uint64_t batch, void *stream) {
+    if (!seeds && batch) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null seed array");
+    return on_device(ctx, [&](tb::Context &c) {
+        if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
+        return tb::encrypt_symmetric(c, seed8, sk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch,
+                                     S(stream), seeds);
     });
 }
 

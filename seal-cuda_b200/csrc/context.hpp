@@ -122,3 +122,8 @@ int ntt_inverse(const Context &c, const uint64_t *in, uint64_t *out, uint64_t po
                 bool lazy, cudaStream_t s);
 
 }  // namespace tb
+
+// The opaque handle of the C ABI (include/troy_b200.h) around one parameter context.
+struct tb_context {
+    tb::Context *c;
+};

@@ -376,17 +376,27 @@ int keygen_secret(Context &c, const uint64_t *seed8, uint64_t *sk, cudaStream_t 
     return status_from(transform<true>(c, sk, 1, 0, K, false, s));
 }
 
+__global__ void seeded_uniform_kernel(uint64_t *c1, const Mod *__restrict__ mods, int L, uint32_t n, uint64_t seed);
+
 // `count` symmetric encryptions of zero at level L in NTT (ntt=1) or coefficient form
 // into out[b] ([2][L][N] at out + b*ostride). Every encryption creates its PRNGs from
 // the factory (encryptZeroSymmetric, src/utils/rlwe.cpp:232-357).
+//
+// seeds != nullptr (host array of `count` words): the seed-compressed form of the
+// reference's GPU path (util::encryptZeroSymmetric, src/utils/rlwe_cuda.cu:262-331).
+// The PRNG keyed by the public seed gives the 64-bit seed (first 32-bit word << 32) +
+// second word (the next pair if that is zero), c1 is the cuRAND expansion of it that
+// the reference's loader regenerates, and seeds[b] returns it; the call waits for the
+// seeds to reach the host.
 int encrypt_zero_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int L, bool ntt, uint64_t *out,
-                           uint64_t ostride, int count, cudaStream_t s) {
+                           uint64_t ostride, int count, cudaStream_t s, uint64_t *seeds = nullptr) {
     const uint64_t n = c.n;
     if (!ostride) ostride = 2ull * L * n;
-    DevBuf st(s), pub(s), noise(s);
+    DevBuf st(s), pub(s), noise(s), sw(s);
     cudaError_t e = st.alloc(sizeof(PrngState) * count);
     if (e == cudaSuccess) e = pub.alloc(sizeof(PrngState) * count);
     if (e == cudaSuccess) e = noise.alloc(8ull * count * L * n);
+    if (e == cudaSuccess && seeds) e = sw.alloc(16ull * count);
     if (e != cudaSuccess) return status_from(e);
     PrngState *bs = st.as<PrngState>(), *ps = pub.as<PrngState>();
     int r = prng_init(bs, count, seed8, s);
@@ -398,9 +408,32 @@ int encrypt_zero_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk
         r = prng_bytes(bs + b, 64, reinterpret_cast<uint8_t *>(ps + b), s);   // seed is the first member
         if (r != TB_OK) return r;
     }
-    for (int b = 0; b < count; b++) {
-        r = sample_poly(c, SAMPLE_UNIFORM, ps + b, 1, 0, L, out + b * ostride + (uint64_t)L * n, 0, s);
-        if (r != TB_OK) return r;
+    if (seeds) {
+        uint8_t *words = sw.as<uint8_t>();
+        for (int b = 0; b < count; b++) {
+            r = prng_bytes(ps + b, 16, words + 16 * b, s);
+            if (r != TB_OK) return r;
+        }
+        std::vector<uint32_t> host(4ull * count);
+        e = cudaMemcpyAsync(host.data(), words, 16ull * count, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return status_from(e);
+        for (int b = 0; b < count; b++) {
+            const uint32_t *w = &host[4ull * b];
+            uint64_t sd = ((uint64_t)w[0] << 32) + w[1];
+            if (!sd) sd = ((uint64_t)w[2] << 32) + w[3];
+            if (!sd) return set_error(TB_ERR_INVALID_ARGUMENT, "ciphertext PRNG gave a zero seed twice");
+            seeds[b] = sd;
+            seeded_uniform_kernel<<<grid_for(n, 256), 256, 0, s>>>(out + b * ostride + (uint64_t)L * n, c.d_mods, L,
+                                                                   (uint32_t)n, sd);
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return status_from(e);
+    } else {
+        for (int b = 0; b < count; b++) {
+            r = sample_poly(c, SAMPLE_UNIFORM, ps + b, 1, 0, L, out + b * ostride + (uint64_t)L * n, 0, s);
+            if (r != TB_OK) return r;
+        }
     }
     r = sample_poly(c, SAMPLE_CBD, bs, count, 0, L, noise.as<uint64_t>(), 0, s);
     if (r != TB_OK) return r;
@@ -541,14 +574,19 @@ int encrypt(Context &c, const uint64_t *seed8, const uint64_t *pk, int L, const 
 // Symmetric encryption with the secret key at level L (Encryptor::encryptSymmetric).
 int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int L, const uint64_t *plain,
                       uint64_t pstride, uint32_t pcount, uint64_t *out, uint64_t ostride, uint64_t count,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint64_t *seeds) {
     const uint64_t n = c.n;
     if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "encryption needs a scheme context");
+    if (seeds && c.scheme == SCHEME_BGV)
+        return set_error(TB_ERR_UNSUPPORTED,
+                         "seed-compressed BGV ciphertexts are not written: the reference's loader keeps their "
+                         "second polynomial in the NTT domain");
     if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
     if (!sk || !out) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
     if (!count) return TB_OK;
+    if (count > 0x7fffffffull) return set_error(TB_ERR_INVALID_ARGUMENT, "too many ciphertexts in one call");
     if (!ostride) ostride = 2ull * L * n;
-    int r = encrypt_zero_symmetric(c, seed8, sk, L, c.scheme == SCHEME_CKKS, out, ostride, (int)count, s);
+    int r = encrypt_zero_symmetric(c, seed8, sk, L, c.scheme == SCHEME_CKKS, out, ostride, (int)count, s, seeds);
     if (r != TB_OK) return r;
     if (plain) {
         const RnsLevel &lv = c.levels[L];

@@ -1,88 +1,90 @@
-"""Batches of ciphertexts with different ring degrees and modulus chains in one launch.
+"""Batches of ciphertexts with different ring degrees and modulus chains (Python side
+of the C ABI's uneven batches, ``tb_uneven_*`` in include/troy_b200.h).
 
-A batch is split into shape groups (one parameter context each). Every group runs
-its whole pipeline — multiply, relinearize, rotate (apply_galois) — as batched C-ABI
-calls on a stream of its own, so the groups overlap on the device; the fork/join of
-all groups is captured once into a CUDA graph, after which one graph launch runs the
-entire uneven batch. The arithmetic per ciphertext is the same as the one-call-per-
-ciphertext path, so the results are identical word for word.
+A batch is split into shape groups (one parameter context each). The library runs
+every group's pipeline — multiply, relinearize, rotate (apply_galois) — as batched
+calls on a stream of its own, so the groups overlap on the device; ``capture()``
+records that fork/join once as a CUDA graph, after which one graph launch runs the
+entire uneven batch. The arithmetic per ciphertext is the same as the
+one-call-per-ciphertext path, so the results are identical word for word.
 """
 from __future__ import annotations
+
+import ctypes
 
 import torch
 
 import tb_capi
 
 
+class _Group(ctypes.Structure):
+    """tb_uneven_group."""
+    _fields_ = [("ctx", ctypes.c_void_p), ("L", ctypes.c_int), ("count", ctypes.c_uint64),
+                ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("relin_key", ctypes.c_void_p),
+                ("galois_key", ctypes.c_void_p), ("galois_elt", ctypes.c_uint32), ("out", ctypes.c_void_p)]
+
+
 class ShapeGroup:
     """Ciphertext pairs of one parameter set: a, b are [count][2][L][N] device tensors
     (int64 view of uint64 words); rlk and gk the relinearization and Galois keys
-    ([K-1][2][K][N]); elt the Galois element of the rotation."""
+    ([K-1][2][K][N]); elt the Galois element of the rotation. out receives the results."""
 
     def __init__(self, ctx: tb_capi.Context, L: int, a, b, rlk, gk, elt: int):
         self.ctx, self.L, self.a, self.b, self.rlk, self.gk, self.elt = ctx, L, a, b, rlk, gk, elt
-        self.count, n = a.shape[0], ctx.n
-        self.t3 = torch.empty((self.count, 3, L, n), dtype=torch.int64, device=a.device)
-        self.out = torch.empty((self.count, 2, L, n), dtype=torch.int64, device=a.device)
+        self.count = a.shape[0]
+        self.out = torch.empty((self.count, 2, L, ctx.n), dtype=torch.int64, device=a.device)
 
-    def run(self, stream):
-        ctx, L, n, c = self.ctx, self.L, self.ctx.n, self.count
-        ctx("multiply", L, self.a, 0, self.b, 0, self.t3, 0, c, stream)
-        ctx("relinearize", L, self.t3, 0, self.rlk, c, stream)
-        ctx("apply_galois", L, self.elt, self.t3, 3 * L * n, self.out, 0, self.gk, c, stream)
-
-    def run_per_op(self, stream):
-        """The same pipeline one ciphertext per call (the reference's usage pattern)."""
-        ctx, L, n = self.ctx, self.L, self.ctx.n
-        for i in range(self.count):
-            t3, out = self.t3[i:i + 1], self.out[i:i + 1]
-            ctx("multiply", L, self.a[i:i + 1], 0, self.b[i:i + 1], 0, t3, 0, 1, stream)
-            ctx("relinearize", L, t3, 0, self.rlk, 1, stream)
-            ctx("apply_galois", L, self.elt, t3, 3 * L * n, out, 0, self.gk, 1, stream)
+    def descriptor(self):
+        return _Group(self.ctx.h.value if hasattr(self.ctx.h, "value") else self.ctx.h, self.L, self.count,
+                      self.a.data_ptr(), self.b.data_ptr(), self.rlk.data_ptr(), self.gk.data_ptr(), self.elt,
+                      self.out.data_ptr())
 
 
 class UnevenBatch:
-    """All shape groups of one batch: run() issues them on one stream each (joined back
-    to the caller's stream); capture() records that fork/join once as a CUDA graph and
-    replay() then launches the whole batch with a single graph launch."""
+    """All shape groups of one batch (a ``tb_uneven`` handle): run() issues them on one
+    stream each, joined back to the caller's stream; run_per_op() one ciphertext per
+    call; capture() records run() once as a CUDA graph and replay() then launches the
+    whole batch with a single graph launch."""
 
     def __init__(self, groups):
         self.groups = list(groups)
-        self.streams = [torch.cuda.Stream() for _ in self.groups]
-        self.graph = None
+        self._lib = tb_capi.lib()
+        arr = (_Group * len(self.groups))(*[g.descriptor() for g in self.groups])
+        self.h = ctypes.c_void_p()
+        self._lib.tb_uneven_create.argtypes = [ctypes.POINTER(_Group), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        tb_capi.check(self._lib.tb_uneven_create(arr, len(self.groups), ctypes.byref(self.h)))
+        self._lib.tb_uneven_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._lib.tb_uneven_run_per_op.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._lib.tb_uneven_capture.argtypes = [ctypes.c_void_p]
+        self._lib.tb_uneven_replay.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._lib.tb_uneven_destroy.argtypes = [ctypes.c_void_p]
+
+    @staticmethod
+    def _s(stream):
+        return (stream or torch.cuda.current_stream()).cuda_stream
 
     def run(self, stream=None):
-        stream = stream or torch.cuda.current_stream()
-        start = torch.cuda.Event()
-        start.record(stream)
-        ends = []
-        for g, s in zip(self.groups, self.streams):
-            s.wait_event(start)
-            g.run(s)
-            e = torch.cuda.Event()
-            e.record(s)
-            ends.append(e)
-        for e in ends:
-            stream.wait_event(e)
+        tb_capi.check(self._lib.tb_uneven_run(self.h, self._s(stream)))
 
     def run_per_op(self, stream=None):
-        stream = stream or torch.cuda.current_stream()
-        for g in self.groups:
-            g.run_per_op(stream)
+        tb_capi.check(self._lib.tb_uneven_run_per_op(self.h, self._s(stream)))
 
     def capture(self):
-        """Records the batch as one CUDA graph. Run the batch once uncaptured first: the
-        library builds per-element tables on first use."""
-        self.graph = torch.cuda.CUDAGraph()
-        cap = torch.cuda.Stream()
-        cap.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.graph(self.graph, stream=cap, capture_error_mode="relaxed"):
-            self.run(cap)
-        torch.cuda.current_stream().wait_stream(cap)
-        return self.graph
+        tb_capi.check(self._lib.tb_uneven_capture(self.h))
 
-    def replay(self):
-        self.graph.replay()
+    def replay(self, stream=None):
+        tb_capi.check(self._lib.tb_uneven_replay(self.h, self._s(stream)))
+
+    def close(self):
+        if self.h:
+            self._lib.tb_uneven_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     @property
     def count(self):

@@ -84,6 +84,7 @@ void Plaintext::load(std::istream &s) {
 }
 
 void Ciphertext::save(std::ostream &s) const {
+    if (seed_ != 0 && size_ > 2) throw std::invalid_argument("Seed exists but size is not 2.");
     put(s, parms_id_);
     put<bool>(s, ntt_);
     put<std::size_t>(s, size_);
@@ -91,12 +92,15 @@ void Ciphertext::save(std::ostream &s) const {
     put<std::size_t>(s, limbs_);
     put(s, scale_);
     put<std::uint64_t>(s, corr_);
-    put<std::uint64_t>(s, 0);  // seed: never compressed
+    put<std::uint64_t>(s, seed_);
     put<bool>(s, false);       // not a termed ciphertext
-    put_words(s, data_.toHost());
+    auto w = data_.toHost();
+    if (seed_ != 0) w.resize(n_ * limbs_);   // c0 only: c1 is the expansion of the seed
+    put_words(s, w);
 }
 
 void Ciphertext::loadHeader(std::istream &s, bool &terms, std::uint64_t &seed) {
+    seed_ = 0;   // a loaded ciphertext holds both polynomials (CiphertextCuda::load)
     parms_id_ = get<ParmsID>(s);
     ntt_ = get<bool>(s);
     size_ = get<std::size_t>(s);

@@ -611,6 +611,7 @@ bool Ciphertext::isTransparent() const {
 void Ciphertext::fromHost(const std::vector<uint64_t> &v) {
     if (v.size() != size_ * limbs_ * n_) throw std::invalid_argument("data size mismatch");
     data_.fromHost(v.data(), v.size());
+    seed_ = 0;
 }
 
 const uint64_t *KSwitchKeys::key(std::size_t index) const {
@@ -620,6 +621,36 @@ const uint64_t *KSwitchKeys::key(std::size_t index) const {
 }
 
 void KernelProvider::initialize(int device) { cuda_check(cudaSetDevice(device), "cudaSetDevice"); }
+
+// ------------------------------------------------------------------ uneven batches
+
+tb_uneven_group UnevenBatch::group(const SEALContext &context, int level_limbs, std::uint64_t count,
+                                   const std::uint64_t *a, const std::uint64_t *b, const std::uint64_t *relin_key,
+                                   const std::uint64_t *galois_key, std::uint32_t galois_elt, std::uint64_t *out) {
+    context.requireSet();
+    tb_uneven_group g{};
+    g.ctx = context.handle();
+    g.L = level_limbs;
+    g.count = count;
+    g.a = a;
+    g.b = b;
+    g.relin_key = relin_key;
+    g.galois_key = galois_key;
+    g.galois_elt = galois_elt;
+    g.out = out;
+    return g;
+}
+
+UnevenBatch::UnevenBatch(const std::vector<tb_uneven_group> &groups) {
+    check(tb_uneven_create(groups.data(), (int)groups.size(), &h_));
+}
+
+UnevenBatch::~UnevenBatch() { tb_uneven_destroy(h_); }
+
+void UnevenBatch::run(void *stream) { check(tb_uneven_run(h_, stream)); }
+void UnevenBatch::runPerOp(void *stream) { check(tb_uneven_run_per_op(h_, stream)); }
+void UnevenBatch::capture() { check(tb_uneven_capture(h_)); }
+void UnevenBatch::replay(void *stream) { check(tb_uneven_replay(h_, stream)); }
 
 // ------------------------------------------------------------------ keys
 
@@ -726,7 +757,7 @@ static int limbs_of(const SEALContext &c, const ParmsID &id, const char *what) {
 }
 
 // EncryptorCuda::encryptInternal (src/encryptor_cuda.cu:92-237).
-void Encryptor::run(const Plaintext *plain, const ParmsID &id, bool asym, Ciphertext &dest) const {
+void Encryptor::run(const Plaintext *plain, const ParmsID &id, bool asym, Ciphertext &dest, bool seeded) const {
     context_.requireSet();
     if (asym && !has_pk_) throw std::logic_error("public key is not set");
     if (!asym && !has_sk_) throw std::logic_error("secret key is not set");
@@ -749,14 +780,19 @@ void Encryptor::run(const Plaintext *plain, const ParmsID &id, bool asym, Cipher
     const uint64_t *seed = context_.keyParms().randomGenerator()->seedPtr();
     const uint64_t *p = plain ? plain->data() : nullptr;
     const uint64_t count = plain ? (ckks ? 0 : plain->coeffCount()) : 0;
+    std::uint64_t ct_seed = 0;
     if (asym)
         check(tb_encrypt(context_.handle(), seed, pk_.data().get(), L, p, 0, count, out.data(), 0, 1, nullptr));
+    else if (seeded)
+        check(tb_encrypt_symmetric_seeded(context_.handle(), seed, sk_.data().get(), L, p, 0, count, out.data(), 0,
+                                          &ct_seed, 1, nullptr));
     else
         check(tb_encrypt_symmetric(context_.handle(), seed, sk_.data().get(), L, p, 0, count, out.data(), 0, 1,
                                    nullptr));
     out.isNttForm() = ckks;
     out.scale() = (plain && ckks) ? plain->scale() : 1.0;
     out.correctionFactor() = 1;
+    out.seed() = ct_seed;
     dest = std::move(out);
 }
 
@@ -766,6 +802,12 @@ void Encryptor::encryptSymmetric(const Plaintext &plain, Ciphertext &dest) const
     run(&plain, parmsIDZero, false, dest);
 }
 void Encryptor::encryptZeroSymmetric(const ParmsID &id, Ciphertext &dest) const { run(nullptr, id, false, dest); }
+void Encryptor::encryptSymmetricSeeded(const Plaintext &plain, Ciphertext &dest) const {
+    run(&plain, parmsIDZero, false, dest, true);
+}
+void Encryptor::encryptZeroSymmetricSeeded(const ParmsID &id, Ciphertext &dest) const {
+    run(nullptr, id, false, dest, true);
+}
 
 // DecryptorCuda::decrypt (src/decryptor_cuda.cu:92-328).
 void Decryptor::decrypt(const Ciphertext &ct, Plaintext &dest) {

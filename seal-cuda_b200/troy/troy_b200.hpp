@@ -312,6 +312,7 @@ public:
         if ((size < 2 && size != 0) || size > 16) throw std::invalid_argument("invalid size");
         data_.resize(size * limbs_ * n_);
         size_ = size;
+        seed_ = 0;
     }
     void reserve(std::size_t) {}
     std::size_t size() const { return size_; }
@@ -325,16 +326,29 @@ public:
     double scale() const { return scale_; }
     std::uint64_t &correctionFactor() { return corr_; }
     std::uint64_t correctionFactor() const { return corr_; }
-    std::uint64_t *data() { return data_.get(); }
+    // Non-zero for a seed-compressed symmetric encryption (Encryptor::
+    // encryptSymmetricSeeded): c1 is the cuRAND expansion of this seed, and save() writes
+    // c0 and the seed only (CiphertextCuda::seed, src/ciphertext_cuda.cuh). Any write
+    // access to the words (the non-const data() accessors, resize, fromHost) clears it,
+    // as the reference's evaluator clears the seed of every ciphertext it writes.
+    std::uint64_t &seed() { return seed_; }
+    std::uint64_t seed() const { return seed_; }
+    std::uint64_t *data() {
+        seed_ = 0;
+        return data_.get();
+    }
     const std::uint64_t *data() const { return data_.get(); }
-    std::uint64_t *data(std::size_t poly) { return data_.get() + poly * limbs_ * n_; }
+    std::uint64_t *data(std::size_t poly) {
+        seed_ = 0;
+        return data_.get() + poly * limbs_ * n_;
+    }
     const std::uint64_t *data(std::size_t poly) const { return data_.get() + poly * limbs_ * n_; }
     std::vector<std::uint64_t> toHost() const { return data_.toHost(); }
     void fromHost(const std::vector<std::uint64_t> &v);
     // Wire format of CiphertextCuda::save/load/saveTerms/loadTerms
-    // (src/ciphertext_cuda.cu:8-185). Seed-compressed ciphertexts are not produced,
-    // and loading one is rejected: the reference expands their second polynomial
-    // with cuRAND.
+    // (src/ciphertext_cuda.cu:8-185). A ciphertext with a seed travels as c0 plus the
+    // seed; loading one needs the context (the second polynomial is regenerated with
+    // cuRAND as the reference's loader does).
     void save(std::ostream &stream) const;
     void load(std::istream &stream);
     void load(std::istream &stream, const SEALContext &context);
@@ -349,6 +363,7 @@ private:
     ParmsID parms_id_ = {0, 0, 0, 0};
     double scale_ = 1.0;
     std::uint64_t corr_ = 1;
+    std::uint64_t seed_ = 0;
 };
 
 class SecretKey {
@@ -475,11 +490,18 @@ public:
     void encryptZero(Ciphertext &destination) const { encryptZero(context_.firstParmsID(), destination); }
     void encryptZero(const ParmsID &parms_id, Ciphertext &destination) const;
     void encryptSymmetric(const Plaintext &plain, Ciphertext &destination) const;
+    // The seed-compressed symmetric encryption of the reference's GPU path
+    // (EncryptorCuda::encryptSymmetric, src/encryptor_cuda.cuh:269-371): destination.seed()
+    // is set and c1 is its cuRAND expansion, so save() writes half the words. BFV and
+    // CKKS (the reference's loader cannot expand a BGV one).
+    void encryptSymmetricSeeded(const Plaintext &plain, Ciphertext &destination) const;
+    void encryptZeroSymmetricSeeded(const ParmsID &parms_id, Ciphertext &destination) const;
     void encryptZeroSymmetric(Ciphertext &destination) const { encryptZeroSymmetric(context_.firstParmsID(), destination); }
     void encryptZeroSymmetric(const ParmsID &parms_id, Ciphertext &destination) const;
 
 private:
-    void run(const Plaintext *plain, const ParmsID &id, bool asym, Ciphertext &destination) const;
+    void run(const Plaintext *plain, const ParmsID &id, bool asym, Ciphertext &destination,
+             bool seeded = false) const;
     const SEALContext &context_;
     PublicKey pk_;
     SecretKey sk_;
@@ -617,6 +639,30 @@ private:
 // Legacy kernel-provider entry of the reference (src/kernelprovider.cuh:13-21): selects device 0.
 struct KernelProvider {
     static void initialize(int device = 0);
+};
+
+// Uneven batches (no counterpart in the reference, which evaluates one ciphertext per
+// call): shape groups of ciphertext pairs of different contexts through multiply ->
+// relinearize -> one rotation, each group batched on a stream of its own, the whole
+// fork/join replayable as one CUDA graph. An RAII owner of the C ABI's tb_uneven
+// (include/troy_b200.h); group() makes a shape group from a context's handle, its
+// keys and device buffers ([count][2][L][n] words each).
+class UnevenBatch {
+public:
+    static tb_uneven_group group(const SEALContext &context, int level_limbs, std::uint64_t count,
+                                 const std::uint64_t *a, const std::uint64_t *b, const std::uint64_t *relin_key,
+                                 const std::uint64_t *galois_key, std::uint32_t galois_elt, std::uint64_t *out);
+    explicit UnevenBatch(const std::vector<tb_uneven_group> &groups);
+    ~UnevenBatch();
+    UnevenBatch(const UnevenBatch &) = delete;
+    UnevenBatch &operator=(const UnevenBatch &) = delete;
+    void run(void *stream = nullptr);
+    void runPerOp(void *stream = nullptr);
+    void capture();
+    void replay(void *stream = nullptr);
+
+private:
+    tb_uneven *h_ = nullptr;
 };
 
 }  // namespace troyn

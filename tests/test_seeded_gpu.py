@@ -95,3 +95,89 @@ def test_ckks_seeded_ciphertext_from_the_reference_loads_and_decrypts():
     keygen = pytroy.KeyGenerator(ctx)
     got = pytroy.CKKSEncoder(ctx).decode(pytroy.Decryptor(ctx, keygen.secret_key()).decrypt(ct))
     assert np.abs(got - reals).max() < 1e-5
+
+
+def _ref_gpu_load(args):
+    """Child process: the reference CUDA build loads bytes made here with its own loader,
+    decrypts them with the secret key of the same seeded factory and decodes."""
+    scheme, n, moduli, t, blob, nvalues = args
+    lib = ctypes.CDLL(REF_GPU)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    lib.ref_gpu_load_decrypt.argtypes = [ctypes.c_int, ctypes.c_size_t, u64p, ctypes.c_int, ctypes.c_uint64, u64p,
+                                         ctypes.c_char_p, ctypes.c_size_t, u64p, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.c_size_t, u64p]
+    L = len(moduli) - 1
+    mods = (ctypes.c_uint64 * len(moduli))(*moduli)
+    seed = (ctypes.c_uint64 * 8)(*SEED)
+    vals = (ctypes.c_uint64 * nvalues)()
+    reals = (ctypes.c_double * nvalues)()
+    words = (ctypes.c_uint64 * (2 * L * n))()
+    rc = lib.ref_gpu_load_decrypt(scheme, n, mods, len(moduli), t, seed, blob, len(blob), vals, reals, nvalues, words)
+    return (rc, np.frombuffer(bytes(vals), np.uint64).copy(), np.frombuffer(bytes(reals), np.float64).copy(),
+            np.frombuffer(bytes(words), np.uint64).copy())
+
+
+def _in_reference(args):
+    with mp.get_context("spawn").Pool(1) as pool:
+        return pool.apply(_ref_gpu_load, (args,))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference CUDA build not present")
+@pytest.mark.parametrize("scheme", ["bfv", "ckks"])
+def test_seeded_ciphertext_written_here_loads_and_decrypts_in_the_reference(scheme):
+    """encrypt_symmetric_seeded writes c0 plus a seed; the reference's own loader
+    regenerates the same second polynomial from the seed and its decryptor recovers the
+    values. The bytes also load back here to the same words."""
+    if scheme == "bfv":
+        n, bits, t = 4096, [36, 36, 37], 65537
+        st = pytroy.SchemeType.bfv
+    else:
+        n, bits, t = 8192, [60, 40, 60], 0
+        st = pytroy.SchemeType.ckks
+    ctx = _context(st, n, bits, t if t else None)
+    moduli = [m.value() for m in pytroy.CoeffModulus.create(n, bits)]
+    L = len(bits) - 1
+    keygen = pytroy.KeyGenerator(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.secret_key())
+    rng = np.random.default_rng(71)
+    if scheme == "bfv":
+        values = rng.integers(0, t, n, dtype=np.uint64)
+        plain = pytroy.BatchEncoder(ctx).encode(values)
+        count = n
+    else:
+        reals = rng.uniform(-1, 1, n // 2)
+        plain = pytroy.CKKSEncoder(ctx).encode(reals, 2.0 ** 40)
+        count = n // 2
+    ct = encryptor.encrypt_symmetric_seeded(plain)
+    assert ct.seed() != 0
+    words = np.asarray(ct.data(), np.uint64)
+    blob = ct.save()
+    assert len(blob) < 8 * L * n + 1024             # c0 and the seed only
+    rc, vals, got_reals, ref_words = _in_reference((1 if scheme == "bfv" else 2, n, moduli, t, blob, count))
+    assert rc in (0, 2)                              # 2: a pending CUDA error of the reference, results kept
+    assert np.array_equal(ref_words, words)          # the reference regenerated the same c1
+    dec = pytroy.Decryptor(ctx, keygen.secret_key())
+    back = pytroy.Ciphertext()
+    back.load(blob, ctx)
+    assert back.seed() == 0 and np.array_equal(np.asarray(back.data(), np.uint64), words)
+    if scheme == "bfv":
+        assert np.array_equal(vals, values)
+        assert np.array_equal(pytroy.BatchEncoder(ctx).decode(dec.decrypt(back)), values)
+    else:
+        assert np.abs(got_reals - reals).max() < 1e-5
+        assert np.abs(pytroy.CKKSEncoder(ctx).decode(dec.decrypt(back)) - reals).max() < 1e-5
+    # an evaluation clears the seed: the result travels in full
+    ev = pytroy.Evaluator(ctx)
+    ev.add_inplace(ct, ct)
+    assert ct.seed() == 0 and len(ct.save()) > 16 * L * n
+
+
+def test_seeded_bgv_encryption_is_refused():
+    n, bits = 4096, [36, 36, 37]
+    t = pytroy.PlainModulus.batching(n, 20)
+    ctx = _context(pytroy.SchemeType.bgv, n, bits, t)
+    keygen = pytroy.KeyGenerator(ctx)
+    encryptor = pytroy.Encryptor(ctx, keygen.secret_key())
+    plain = pytroy.BatchEncoder(ctx).encode(np.zeros(n, np.uint64))
+    with pytest.raises(Exception, match="NTT domain"):
+        encryptor.encrypt_symmetric_seeded(plain)
