@@ -412,6 +412,11 @@ int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflie
    value; 0 restores the default). */
 int tb_keyswitch_set_budget(uint64_t bytes);
 uint64_t tb_keyswitch_get_budget(void);
+/* Key switching (relinearize, rotations) of degrees 4096 .. 16384 through one persistent
+   launch per step (CTAs that take the next limb from a device counter) instead of one CTA
+   per limb; the same words either way. Off by default. No counterpart in the reference. */
+int tb_keyswitch_set_persistent(int on);
+int tb_keyswitch_get_persistent(void);
 
 /* ----------------------------------------------------------- uneven batches */
 
@@ -450,6 +455,10 @@ int tb_uneven_run_per_op(tb_uneven *batch, void *stream);
 int tb_uneven_capture(tb_uneven *batch);
 /* One graph launch of the whole captured batch on `stream`. */
 int tb_uneven_replay(tb_uneven *batch, void *stream);
+/* on != 0: after the groups' products (one stream each), the relinearizations and the
+   rotations of every group run with one persistent launch per key-switch step for all
+   groups (at most 8 groups, degrees 4096 .. 16384; set before capture). Same words. */
+int tb_uneven_set_shapes(tb_uneven *batch, int on);
 int tb_uneven_destroy(tb_uneven *batch);
 
 /* ---------------------------------------------------------------- tracing */

@@ -25,6 +25,7 @@
 
 namespace tb {
 size_t ks_scratch_budget();
+bool ks_persistent();
 
 unsigned grid_for(uint64_t work, int threads);
 
@@ -54,6 +55,19 @@ struct KeyGroups {
         r.first[r.count] = nb;
         return r;
     }
+};
+
+// One shape of a multi-shape key switch: B ciphertexts of context c at level L, target
+// [B][L][N] at target + b*tstride, ciphertext (2 polys, L limbs) at ct + b*cstride.
+struct KsShape {
+    const Context *c;
+    int L;
+    const uint64_t *target;
+    uint64_t tstride;
+    uint64_t *ct;
+    uint64_t cstride;
+    KeyGroups keys;
+    uint64_t B;
 };
 
 namespace {
@@ -156,15 +170,12 @@ struct ModUpOp {
     }
 };
 
-// Step 3: acc[b][c][i] = sum_j digit(b, j, i) * key[j][c][mi] mod q_mi, two coefficients per thread.
-__global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
-                                uint64_t tstride, KeyGroups keys, uint64_t *__restrict__ acc,
-                                const Mod *__restrict__ mods, int L, int K, int ckks, int logn) {
-    const uint32_t n = 1u << logn;
-    const uint32_t e = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (e >= n) return;
-    const int i = blockIdx.y;
-    const size_t cb = blockIdx.z;
+// Step 3: acc[b][c][i] = sum_j digit(b, j, i) * key[j][c][mi] mod q_mi, two coefficients
+// (e, e+1) of output modulus i of ciphertext cb per thread.
+__device__ __forceinline__ void ks_inner_pair(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
+                                              uint64_t tstride, const KeyGroups &keys, uint64_t *__restrict__ acc,
+                                              const Mod *__restrict__ mods, int L, int K, int ckks, int logn,
+                                              uint32_t e, int i, size_t cb) {
     const int mi = i == L ? K - 1 : i;
     const Mod m = mods[mi];
     const uint64_t *__restrict__ key = keys.of((uint32_t)cb);
@@ -187,6 +198,48 @@ __global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint6
     uint64_t *o1 = acc + (((cb * 2 + 1) * (L + 1) + i) << logn) + e;
     *reinterpret_cast<ulonglong2 *>(o0) = make_ulonglong2(reduce128(a00.hi, a00.lo, m), reduce128(a01.hi, a01.lo, m));
     *reinterpret_cast<ulonglong2 *>(o1) = make_ulonglong2(reduce128(a10.hi, a10.lo, m), reduce128(a11.hi, a11.lo, m));
+}
+
+constexpr int INNER_THREADS = 128;
+
+__global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
+                                uint64_t tstride, KeyGroups keys, uint64_t *__restrict__ acc,
+                                const Mod *__restrict__ mods, int L, int K, int ckks, int logn) {
+    const uint32_t e = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (e >= (1u << logn)) return;
+    ks_inner_pair(digits, target, tstride, keys, acc, mods, L, K, ckks, logn, e, blockIdx.y, blockIdx.z);
+}
+
+// The inner products of several key-switch shapes (contexts of different degrees and
+// levels) in one launch: blocks [first[g], first[g+1]) belong to shape g, laid out per
+// ciphertext as (output modulus, coefficient chunk) like the grid of ks_inner_kernel.
+struct InnerShape {
+    const uint64_t *digits, *target;
+    uint64_t tstride;
+    KeyGroups keys;
+    uint64_t *acc;
+    const Mod *mods;
+    int L, K, ckks, logn;
+};
+
+struct InnerTable {
+    int count = 0;
+    InnerShape sh[MAX_SHAPES];
+    unsigned first[MAX_SHAPES + 1];
+};
+
+__global__ void __launch_bounds__(INNER_THREADS) ks_inner_shapes_kernel(InnerTable t) {
+    int g = 0;
+    while (g + 1 < t.count && blockIdx.x >= t.first[g + 1]) g++;
+    const InnerShape &S = t.sh[g];
+    const unsigned local = blockIdx.x - t.first[g];
+    const unsigned chunks = ((1u << S.logn) / 2 + INNER_THREADS - 1) / INNER_THREADS;
+    const unsigned per_ct = chunks * (unsigned)(S.L + 1);
+    const unsigned cb = local / per_ct, r = local - cb * per_ct;
+    const int i = (int)(r / chunks);
+    const uint32_t e = 2 * ((r - (unsigned)i * chunks) * INNER_THREADS + threadIdx.x);
+    if (e >= (1u << S.logn)) return;
+    ks_inner_pair(S.digits, S.target, S.tstride, S.keys, S.acc, S.mods, S.L, S.K, S.ckks, S.logn, e, i, cb);
 }
 
 // Step 4: inverse NTT of the special-prime accumulator; CKKS/BFV add (q_k - 1)/2 for
@@ -343,6 +396,8 @@ struct Scratch {
 
 void ensure_pool_retains(int device);
 
+int keyswitch_shapes(const KsShape *shapes, int count, cudaStream_t s);
+
 // target[b] (L limbs) at target + b*tstride; ct[b] (2 polys, L limbs) at ct + b*cstride.
 int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t tstride, uint64_t *ct,
                      uint64_t cstride, const KeyGroups &keys, uint64_t B, cudaStream_t s) {
@@ -364,6 +419,11 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
     // Whole batches per launch keep every stage's grid several waves deep; the batch is
     // only split when its intermediates would exceed the scratch budget.
     const size_t budget = ks_scratch_budget();
+    if (ks_persistent() && c.logn >= 12 && c.logn <= MAX_LOGB && per_ct * B <= budget &&
+        B <= 0x7fffffffull / ((uint64_t)L * (L + 1))) {
+        const KsShape sh{&c, L, target, tstride, ct, cstride, keys, B};
+        return keyswitch_shapes(&sh, 1, s);
+    }
     uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(B, budget / per_ct));
     ensure_pool_retains(c.device);
     Scratch scr(s);
@@ -420,6 +480,187 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
         }
         if (e != cudaSuccess) return status_from(e);
     }
+    return TB_OK;
+}
+
+// ------------------------------------------------- several shapes in one launch per step
+//
+// Key switching of ciphertexts of several contexts (ring degrees 2^12 .. 2^14, any
+// levels, any of the three schemes) with one persistent launch per step for all of
+// them: the CKKS target inverse transforms, every mod-up transform, every inner
+// product, every special-prime inverse transform, and the mod-downs (one launch per
+// scheme present: the CKKS mod-down is a forward transform, BFV's and BGV's inverse
+// ones with different epilogues). Same operations, same words as keyswitch_groups per
+// shape.
+int keyswitch_shapes(const KsShape *shapes, int count, cudaStream_t s) {
+    if (count < 1 || count > MAX_SHAPES) return set_error(TB_ERR_INVALID_ARGUMENT, "between 1 and 8 shapes");
+    size_t bytes = 0;
+    for (int g = 0; g < count; g++) {
+        const KsShape &sh = shapes[g];
+        const Context &c = *sh.c;
+        const int K = (int)c.chain.size(), L = sh.L;
+        if (c.scheme == SCHEME_RAW) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a scheme context");
+        if (K < 2) return set_error(TB_ERR_UNSUPPORTED, "key switching needs a special prime");
+        if (L < 1 || L > K - 1) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the data chain");
+        if (c.logn < 12 || c.logn > MAX_LOGB)
+            return set_error(TB_ERR_UNSUPPORTED, "one-launch key switching takes degrees 4096 .. 16384");
+        if (!sh.target || !sh.ct || sh.keys.count < 1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+        for (int k = 0; k < sh.keys.count; k++)
+            if (!sh.keys.key[k]) return set_error(TB_ERR_NO_KEY, "missing key-switching key");
+        if (sh.B > 0x7fffffffull / ((uint64_t)L * (L + 1))) return set_error(TB_ERR_INVALID_ARGUMENT, "batch too large");
+        const bool ckks = c.scheme == SCHEME_CKKS;
+        bytes += ((ckks ? (size_t)L : 0) + (size_t)L * (L + 1) + 2ull * (L + 1) + 2) * c.n * 8 * sh.B;
+    }
+    ensure_pool_retains(shapes[0].c->device);
+    Scratch scr(s);
+    cudaError_t e = scr.alloc(bytes + 256);
+    if (e != cudaSuccess) return status_from(e);
+    unsigned *counter = (unsigned *)scr.p;
+    uint64_t *at = (uint64_t *)((char *)scr.p + 256);
+    // largest degree first: the cheap limbs of small rings fill the last round
+    int order[MAX_SHAPES];
+    for (int g = 0; g < count; g++) order[g] = g;
+    std::stable_sort(order, order + count, [&](int a, int b) { return shapes[a].c->logn > shapes[b].c->logn; });
+    struct Bufs {
+        uint64_t *tgt, *digits, *acc, *last;
+    } buf[MAX_SHAPES];
+    for (int k = 0; k < count; k++) {
+        const KsShape &sh = shapes[order[k]];
+        const uint64_t n = sh.c->n, L = (uint64_t)sh.L;
+        const bool ckks = sh.c->scheme == SCHEME_CKKS;
+        buf[k].tgt = at;
+        buf[k].digits = buf[k].tgt + (ckks ? sh.B * L * n : 0);
+        buf[k].acc = buf[k].digits + sh.B * L * (L + 1) * n;
+        buf[k].last = buf[k].acc + sh.B * 2 * (L + 1) * n;
+        at = buf[k].last + sh.B * 2 * n;
+    }
+    // 1. CKKS targets out of the NTT domain
+    {
+        ShapeTable<StridedNttOp<false>> t;
+        unsigned f = 0;
+        for (int k = 0; k < count; k++) {
+            const KsShape &sh = shapes[order[k]];
+            if (sh.c->scheme != SCHEME_CKKS || !sh.B) continue;
+            const uint64_t tstride = sh.tstride ? sh.tstride : (uint64_t)sh.L * sh.c->n;
+            t.op[t.count] = StridedNttOp<false>{sh.target, buf[k].tgt, tstride, (uint64_t)sh.L * sh.c->n,
+                                                sh.c->d_mods, 0, sh.L, 0, sh.c->logn};
+            t.logn[t.count] = sh.c->logn;
+            t.first[t.count] = f;
+            f += (unsigned)(sh.B * sh.L);
+            t.count++;
+        }
+        t.first[t.count] = f;
+        if (t.count) {
+            TraceScope ts("ks_target_intt", s);
+            e = launch_shapes<false>(t, counter, s);
+            if (e != cudaSuccess) return status_from(e);
+        }
+    }
+    // 2. mod-up transforms
+    {
+        ShapeTable<ModUpOp> t;
+        unsigned f = 0;
+        for (int k = 0; k < count; k++) {
+            const KsShape &sh = shapes[order[k]];
+            if (!sh.B) continue;
+            const bool ckks = sh.c->scheme == SCHEME_CKKS;
+            const uint64_t tstride = sh.tstride ? sh.tstride : (uint64_t)sh.L * sh.c->n;
+            t.op[t.count] = ModUpOp{ckks ? buf[k].tgt : sh.target, ckks ? (uint64_t)sh.L * sh.c->n : tstride,
+                                    buf[k].digits, sh.c->d_mods, nullptr, sh.L, (int)sh.c->chain.size(), ckks ? 1 : 0,
+                                    sh.c->logn};
+            t.logn[t.count] = sh.c->logn;
+            t.first[t.count] = f;
+            f += (unsigned)(sh.B * (ckks ? sh.L * sh.L : sh.L * (sh.L + 1)));
+            t.count++;
+        }
+        t.first[t.count] = f;
+        if (t.count) {
+            TraceScope ts("ks_modup_ntt", s);
+            e = launch_shapes<true>(t, counter, s);
+            if (e != cudaSuccess) return status_from(e);
+        }
+    }
+    // 3. inner products
+    {
+        InnerTable t;
+        unsigned f = 0;
+        for (int k = 0; k < count; k++) {
+            const KsShape &sh = shapes[order[k]];
+            if (!sh.B) continue;
+            const uint64_t tstride = sh.tstride ? sh.tstride : (uint64_t)sh.L * sh.c->n;
+            t.sh[t.count] = InnerShape{buf[k].digits, sh.target, tstride, sh.keys, buf[k].acc, sh.c->d_mods, sh.L,
+                                       (int)sh.c->chain.size(), sh.c->scheme == SCHEME_CKKS ? 1 : 0, sh.c->logn};
+            t.first[t.count] = f;
+            const unsigned chunks = (sh.c->n / 2 + INNER_THREADS - 1) / INNER_THREADS;
+            f += (unsigned)(sh.B * (sh.L + 1)) * chunks;
+            t.count++;
+        }
+        t.first[t.count] = f;
+        if (t.count && f) {
+            TraceScope ts("ks_inner_product", s);
+            ks_inner_shapes_kernel<<<f, INNER_THREADS, 0, s>>>(t);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return status_from(e);
+        }
+    }
+    // 4. special-prime accumulators out of the NTT domain
+    {
+        ShapeTable<SpecialInttOp> t;
+        unsigned f = 0;
+        for (int k = 0; k < count; k++) {
+            const KsShape &sh = shapes[order[k]];
+            if (!sh.B) continue;
+            t.op[t.count] = SpecialInttOp{buf[k].acc, buf[k].last, sh.c->d_mods, sh.L, (int)sh.c->chain.size(),
+                                          sh.c->scheme == SCHEME_BGV ? 1 : 0, sh.c->logn};
+            t.logn[t.count] = sh.c->logn;
+            t.first[t.count] = f;
+            f += (unsigned)(sh.B * 2);
+            t.count++;
+        }
+        t.first[t.count] = f;
+        if (t.count) {
+            TraceScope ts("ks_special_intt", s);
+            e = launch_shapes<false>(t, counter, s);
+            if (e != cudaSuccess) return status_from(e);
+        }
+    }
+    // 5. mod-down into the ciphertexts, one launch per scheme present
+    TraceScope ts("ks_moddown", s);
+    ShapeTable<ModDownCkksOp> tc;
+    ShapeTable<ModDownBfvOp> tf;
+    ShapeTable<ModDownBgvOp> tg;
+    unsigned fc = 0, ff = 0, fg = 0;
+    for (int k = 0; k < count; k++) {
+        const KsShape &sh = shapes[order[k]];
+        if (!sh.B) continue;
+        const Context &c = *sh.c;
+        const int K = (int)c.chain.size();
+        const uint64_t cstride = sh.cstride ? sh.cstride : 2ull * sh.L * c.n;
+        const ModDownBase mb{buf[k].acc, buf[k].last, sh.ct, cstride, c.d_mods, c.d_drop, sh.L, K, c.logn};
+        const unsigned limbs = (unsigned)(sh.B * 2 * sh.L);
+        if (c.scheme == SCHEME_CKKS) {
+            tc.op[tc.count] = ModDownCkksOp{mb};
+            tc.logn[tc.count] = c.logn;
+            tc.first[tc.count++] = fc;
+            fc += limbs;
+        } else if (c.scheme == SCHEME_BFV) {
+            tf.op[tf.count] = ModDownBfvOp{mb};
+            tf.logn[tf.count] = c.logn;
+            tf.first[tf.count++] = ff;
+            ff += limbs;
+        } else {
+            tg.op[tg.count] = ModDownBgvOp{mb, c.t_mod, c.inv_qlast_t[K]};
+            tg.logn[tg.count] = c.logn;
+            tg.first[tg.count++] = fg;
+            fg += limbs;
+        }
+    }
+    tc.first[tc.count] = fc;
+    tf.first[tf.count] = ff;
+    tg.first[tg.count] = fg;
+    if (tc.count && (e = launch_shapes<true>(tc, counter, s)) != cudaSuccess) return status_from(e);
+    if (tf.count && (e = launch_shapes<false>(tf, counter, s)) != cudaSuccess) return status_from(e);
+    if (tg.count && (e = launch_shapes<false>(tg, counter, s)) != cudaSuccess) return status_from(e);
     return TB_OK;
 }
 
@@ -602,6 +843,71 @@ int apply_galois_groups(Context &c, int L, int groups, const uint32_t *elts, con
         if (e != cudaSuccess) return status_from(e);
     }
     return TB_OK;
+}
+
+// The relinearize -> rotate part of an uneven batch with every key-switch step in one
+// launch for all shapes: t3[g] holds shape g's B products ([B][3][L][n]); they are
+// relinearized in place (one keyswitch_shapes), each shape's Galois permutation writes
+// out[g] (c0 permuted, c1 cleared) and its permuted c1 into scratch, and one more
+// keyswitch_shapes adds the rotation key switch into out[g] (applyGaloisInplace,
+// src/evaluator.cpp:2153-2249, for every shape at once).
+int uneven_relin_rotate(Context *const *ctxs, const int *Ls, const uint64_t *Bs, uint64_t *const *t3,
+                        const uint64_t *const *rlks, const uint64_t *const *gks, const uint32_t *elts,
+                        uint64_t *const *outs, int count, cudaStream_t s) {
+    if (count < 1 || count > MAX_SHAPES) return set_error(TB_ERR_INVALID_ARGUMENT, "between 1 and 8 shapes");
+    KsShape sh[MAX_SHAPES];
+    uint64_t words = 0;
+    for (int g = 0; g < count; g++) {
+        const uint64_t n = ctxs[g]->n, L = (uint64_t)Ls[g];
+        KeyGroups kg;
+        kg.count = 1;
+        kg.key[0] = rlks[g];
+        kg.first[0] = 0;
+        kg.first[1] = (uint32_t)Bs[g];
+        sh[g] = KsShape{ctxs[g], Ls[g], t3[g] + 2 * L * n, 3 * L * n, t3[g], 3 * L * n, kg, Bs[g]};
+        words += Bs[g] * L * n;
+    }
+    int st = keyswitch_shapes(sh, count, s);
+    if (st != TB_OK) return st;
+    ensure_pool_retains(ctxs[0]->device);
+    Scratch scr(s);
+    cudaError_t e = scr.alloc(words * 8);
+    if (e != cudaSuccess) return status_from(e);
+    uint64_t *tgt = (uint64_t *)scr.p;
+    {
+        TraceScope ts("galois_permute", s);
+        for (int g = 0; g < count; g++) {
+            Context &c = *ctxs[g];
+            const uint64_t n = c.n, L = (uint64_t)Ls[g];
+            GaloisGroups gg;
+            gg.count = 1;
+            gg.elt[0] = elts[g];
+            gg.perm[0] = nullptr;
+            gg.first[0] = 0;
+            gg.first[1] = (uint32_t)Bs[g];
+            if (c.scheme == SCHEME_CKKS) {
+                st = galois_ntt_table(c, elts[g], &gg.perm[0]);
+                if (st != TB_OK) return st;
+            }
+            dim3 grid((unsigned)((n + 255) / 256), (unsigned)L, (unsigned)Bs[g]);
+            if (c.scheme == SCHEME_CKKS)
+                galois_ntt_kernel<<<grid, 256, 0, s>>>(t3[g], 3 * L * n, outs[g], 2 * L * n, tgt, L * n,
+                                                       outs[g] + L * n, gg, (int)L, c.logn);
+            else
+                galois_coeff_kernel<<<grid, 256, 0, s>>>(t3[g], 3 * L * n, outs[g], 2 * L * n, tgt, L * n,
+                                                         outs[g] + L * n, c.d_mods, (int)L, c.logn, gg);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return status_from(e);
+            KeyGroups kg;
+            kg.count = 1;
+            kg.key[0] = gks[g];
+            kg.first[0] = 0;
+            kg.first[1] = (uint32_t)Bs[g];
+            sh[g] = KsShape{ctxs[g], Ls[g], tgt, L * n, outs[g], 2 * L * n, kg, Bs[g]};
+            tgt += Bs[g] * L * n;
+        }
+    }
+    return keyswitch_shapes(sh, count, s);
 }
 
 int apply_galois(Context &c, int L, uint32_t elt, const uint64_t *in, uint64_t istride, uint64_t *out,

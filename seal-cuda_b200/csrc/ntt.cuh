@@ -21,6 +21,7 @@
 
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
@@ -185,18 +186,23 @@ __device__ __forceinline__ void fwd_copy_out(const Op &op, const Ctx &c, const u
     }
 }
 
-template <int LOGB, int V, class Op>
-__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op, int s0) {
-    extern __shared__ uint64_t sm[];
+// One limb (or sub-block) b of Op by a CTA of T threads, starting at global stage s0.
+template <int LOGB, int T, class Op>
+__device__ __forceinline__ void ntt_fwd_limb(const Op &op, int limb, int s0, uint64_t *sm) {
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB, V>::THREADS;
-    constexpr int REM = NttCfg<LOGB, V>::REM;
-    const auto c = op.ctx(blockIdx.x);
+    constexpr int REM = LOGB % 3;
+    const auto c = op.ctx(limb);
     const uint32_t rbase = (1u << s0) + c.lm.sb;
     constexpr int FIRST = REM != 0 ? REM : 3;
     fwd_pass<FIRST, true, LOGB, T, 0, false>(op, c, sm, rbase);
     fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
     fwd_copy_out<NB, T>(op, c, sm, 0);   // coalesced, two coefficients per thread
+}
+
+template <int LOGB, int V, class Op>
+__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op, int s0) {
+    extern __shared__ uint64_t sm[];
+    ntt_fwd_limb<LOGB, NttCfg<LOGB, V>::THREADS>(op, blockIdx.x, s0, sm);
 }
 
 // ---------------------------------------------------------------- inverse
@@ -276,14 +282,13 @@ __device__ __forceinline__ void inv_passes(const Op &op, const Ctx &c, uint64_t 
     }
 }
 
-// scale_last: this CTA's last stage is the transform's last stage (whole limb).
-template <int LOGB, int V, class Op>
-__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op, int logn, int scale_last) {
-    extern __shared__ uint64_t sm[];
+// One limb (or sub-block) b of Op by a CTA of T threads; scale_last: this CTA's last
+// stage is the transform's last stage (whole limb).
+template <int LOGB, int T, class Op>
+__device__ __forceinline__ void ntt_inv_limb(const Op &op, int limb, int logn, int scale_last, uint64_t *sm) {
     constexpr int NB = 1 << LOGB;
-    constexpr int T = NttCfg<LOGB, V>::THREADS;
-    constexpr int REM = NttCfg<LOGB, V>::REM;
-    const auto c = op.ctx(blockIdx.x);
+    constexpr int REM = LOGB % 3;
+    const auto c = op.ctx(limb);
     for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
         uint64_t a, b;
         op.load2(c, e, a, b);
@@ -299,6 +304,12 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op
     inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, logn);
     if (scale_last) inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
     else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
+}
+
+template <int LOGB, int V, class Op>
+__global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_inv_kernel(Op op, int logn, int scale_last) {
+    extern __shared__ uint64_t sm[];
+    ntt_inv_limb<LOGB, NttCfg<LOGB, V>::THREADS>(op, blockIdx.x, logn, scale_last, sm);
 }
 
 // ---------------------------------------------------------------- two-CTA limbs
@@ -634,6 +645,79 @@ inline cudaError_t launch_ntt(const Op &op, unsigned blocks, int s0_or_logn, int
     } else {
         return launch_inv<LOGB, V>(op, blocks, s0_or_logn, scale_last, s);
     }
+}
+
+// ---------------------------------------------------------------- several shapes, one launch
+// Whole limbs of up to MAX_SHAPES groups of ring degrees 2^12 .. 2^14, each group with
+// its own Op (context tables, buffers, level), transformed by one persistent launch: as
+// many CTAs of 1024 threads as the SMs hold at once, each taking the next limb from a
+// device counter until every limb of every group is done (no CTA waits on another).
+// Groups come largest degree first, so the cheap limbs of the small rings fill the last
+// round of the large ones. A limb runs exactly as in the one-CTA kernels (same passes,
+// same butterflies), only with 1024 threads at every degree.
+constexpr int MAX_SHAPES = 8;
+constexpr int SHAPE_THREADS = 1024;
+
+template <class Op>
+struct ShapeTable {
+    int count = 0;
+    Op op[MAX_SHAPES];
+    int logn[MAX_SHAPES];
+    unsigned first[MAX_SHAPES + 1];   // limbs of group g: items first[g] .. first[g+1]-1
+};
+
+template <bool FWD, class Op>
+__global__ void __launch_bounds__(SHAPE_THREADS) ntt_shapes_kernel(ShapeTable<Op> t, unsigned *counter) {
+    extern __shared__ uint64_t sm[];
+    __shared__ unsigned next;
+    const unsigned total = t.first[t.count];
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1u);
+        __syncthreads();
+        const unsigned item = next;
+        __syncthreads();   // every thread has the item before thread 0 takes the next one
+        if (item >= total) return;
+        int g = 0;
+        while (g + 1 < t.count && item >= t.first[g + 1]) g++;
+        const Op op = t.op[g];
+        const int limb = (int)(item - t.first[g]);
+        if constexpr (FWD) {
+            if (t.logn[g] == 14) ntt_fwd_limb<14, SHAPE_THREADS>(op, limb, 0, sm);
+            else if (t.logn[g] == 13) ntt_fwd_limb<13, SHAPE_THREADS>(op, limb, 0, sm);
+            else ntt_fwd_limb<12, SHAPE_THREADS>(op, limb, 0, sm);
+        } else {
+            if (t.logn[g] == 14) ntt_inv_limb<14, SHAPE_THREADS>(op, limb, 14, 1, sm);
+            else if (t.logn[g] == 13) ntt_inv_limb<13, SHAPE_THREADS>(op, limb, 13, 1, sm);
+            else ntt_inv_limb<12, SHAPE_THREADS>(op, limb, 12, 1, sm);
+        }
+        __syncthreads();   // shared memory free for the next limb
+    }
+}
+
+// counter: one device word, zeroed here before the launch (stream-ordered).
+template <bool FWD, class Op>
+inline cudaError_t launch_shapes(const ShapeTable<Op> &t, unsigned *counter, cudaStream_t s) {
+    if (t.count < 1 || t.count > MAX_SHAPES || !counter) return cudaErrorInvalidValue;
+    int maxlog = 0;
+    for (int g = 0; g < t.count; g++) {
+        if (t.logn[g] < 12 || t.logn[g] > MAX_LOGB) return cudaErrorInvalidValue;
+        maxlog = t.logn[g] > maxlog ? t.logn[g] : maxlog;
+    }
+    const unsigned total = t.first[t.count];
+    if (!total) return cudaSuccess;
+    const size_t smem = sizeof(uint64_t) << maxlog;
+    auto k = ntt_shapes_kernel<FWD, Op>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(8 << MAX_LOGB));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, SHAPE_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const unsigned grid = std::min<unsigned>(total, (unsigned)(sm_count() * per_sm));
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    k<<<grid, SHAPE_THREADS, smem, s>>>(t, counter);
+    return cudaGetLastError();
 }
 
 // A launch of at most half as many limbs as the device has SMs leaves most SMs idle with

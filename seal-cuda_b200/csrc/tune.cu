@@ -40,6 +40,11 @@ int ntt_variant(bool fwd, int logb) {
     return g_variant[fwd ? 1 : 0][logb].load(std::memory_order_relaxed);
 }
 
+// Key switching of one context through the persistent one-launch-per-step form
+// (keyswitch_shapes) instead of one CTA per limb (tb_keyswitch_set_persistent).
+std::atomic<int> g_ks_persistent{0};
+bool ks_persistent() { return g_ks_persistent.load(std::memory_order_relaxed) != 0; }
+
 size_t ks_scratch_budget() {
     unsigned long long v = g_ks_budget.load(std::memory_order_relaxed);
     if (v) return (size_t)v;
@@ -215,5 +220,12 @@ int tb_keyswitch_set_budget(uint64_t bytes) {
 }
 
 uint64_t tb_keyswitch_get_budget(void) { return tb::ks_scratch_budget(); }
+
+int tb_keyswitch_set_persistent(int on) {
+    tb::g_ks_persistent.store(on ? 1 : 0);
+    return TB_OK;
+}
+
+int tb_keyswitch_get_persistent(void) { return tb::ks_persistent() ? 1 : 0; }
 
 }  // extern "C"

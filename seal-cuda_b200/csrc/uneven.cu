@@ -6,7 +6,10 @@
 // tb_relinearize, tb_apply_galois: one launch sequence per stage for every
 // ciphertext of the group) issued on a stream of its own, so the groups overlap on the
 // device: a group of small rings fills the SMs a group of large rings leaves idle in
-// its short launches. The fork/join of all groups is recorded once as a CUDA graph
+// its short launches. In the shapes mode (tb_uneven_set_shapes) the products still run
+// per group on their streams, and then the relinearizations and rotations of every
+// group run as one persistent launch per key-switch step for all degrees and levels
+// at once (keyswitch_shapes). Either way the fork/join is recorded once as a CUDA graph
 // (the library's stream-ordered scratch allocations become graph memory nodes), after
 // which one graph launch runs the whole uneven batch. The reference drives these
 // operations one ciphertext per call (EvaluatorCuda::multiply / relinearizeInplace /
@@ -23,6 +26,9 @@
 
 namespace tb {
 int galois_ntt_table(Context &c, uint32_t elt, const uint32_t **out);  // keyswitch.cu
+int uneven_relin_rotate(Context *const *ctxs, const int *Ls, const uint64_t *Bs, uint64_t *const *t3,
+                        const uint64_t *const *rlks, const uint64_t *const *gks, const uint32_t *elts,
+                        uint64_t *const *outs, int count, cudaStream_t s);  // keyswitch.cu
 }
 
 struct tb_uneven {
@@ -35,6 +41,7 @@ struct tb_uneven {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int device = 0;
+    bool shapes = false;   // key switching of all groups in one launch per step
 
     ~tb_uneven() {
         int prev = -1;
@@ -84,7 +91,40 @@ int group_pipeline(const tb_uneven_group &g, uint64_t *t3, bool per_op, cudaStre
     return TB_OK;
 }
 
+// Shapes mode: the groups' products on their own streams (joined back to s), then the
+// relinearizations and rotations of every group with one launch per key-switch step.
+int shapes_pipeline(tb_uneven *u, cudaStream_t s) {
+    cudaError_t e = cudaEventRecord(u->start, s);
+    if (e != cudaSuccess) return tb::status_from(e);
+    const int count = (int)u->groups.size();
+    tb::Context *ctxs[tb::MAX_SHAPES];
+    int Ls[tb::MAX_SHAPES];
+    uint64_t Bs[tb::MAX_SHAPES];
+    uint64_t *outs[tb::MAX_SHAPES];
+    const uint64_t *rlks[tb::MAX_SHAPES], *gks[tb::MAX_SHAPES];
+    uint32_t elts[tb::MAX_SHAPES];
+    for (int g = 0; g < count; g++) {
+        const tb_uneven_group &G = u->groups[g];
+        e = cudaStreamWaitEvent(u->streams[g], u->start, 0);
+        if (e != cudaSuccess) return tb::status_from(e);
+        const int st = tb_multiply(G.ctx, G.L, G.a, 0, G.b, 0, u->t3[g], 0, G.count, u->streams[g]);
+        if (st != TB_OK) return st;
+        e = cudaEventRecord(u->done[g], u->streams[g]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, u->done[g], 0);
+        if (e != cudaSuccess) return tb::status_from(e);
+        ctxs[g] = G.ctx->c;
+        Ls[g] = G.L;
+        Bs[g] = G.count;
+        outs[g] = G.out;
+        rlks[g] = G.relin_key;
+        gks[g] = G.galois_key;
+        elts[g] = G.galois_elt;
+    }
+    return tb::uneven_relin_rotate(ctxs, Ls, Bs, u->t3.data(), rlks, gks, elts, outs, count, s);
+}
+
 int fork_join(tb_uneven *u, cudaStream_t s) {
+    if (u->shapes) return shapes_pipeline(u, s);
     cudaError_t e = cudaEventRecord(u->start, s);
     if (e != cudaSuccess) return tb::status_from(e);
     for (size_t g = 0; g < u->groups.size(); g++) {
@@ -97,6 +137,14 @@ int fork_join(tb_uneven *u, cudaStream_t s) {
         if (e != cudaSuccess) return tb::status_from(e);
     }
     return TB_OK;
+}
+
+// Whether every group can take the one-launch-per-step key switching.
+bool shapes_possible(const tb_uneven *u) {
+    if (u->groups.size() > (size_t)tb::MAX_SHAPES) return false;
+    for (const auto &g : u->groups)
+        if (g.ctx->c->logn < 12 || g.ctx->c->logn > tb::MAX_LOGB || g.count > 0x7fffffffull / 4096) return false;
+    return true;
 }
 
 }  // namespace
@@ -210,6 +258,15 @@ int tb_uneven_replay(tb_uneven *u, void *stream) {
     if (!u->exec) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "uneven batch not captured");
     DeviceGuard guard(u->device);
     return tb::status_from(cudaGraphLaunch(u->exec, reinterpret_cast<cudaStream_t>(stream)));
+}
+
+int tb_uneven_set_shapes(tb_uneven *u, int on) {
+    if (!u) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "null uneven batch");
+    if (on && !shapes_possible(u))
+        return set_error(tb::TB_ERR_UNSUPPORTED, "one-launch key switching takes at most 8 groups of degree 4096 .. 16384");
+    if (u->exec) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "uneven batch already captured");
+    u->shapes = on != 0;
+    return TB_OK;
 }
 
 int tb_uneven_destroy(tb_uneven *u) {

@@ -63,6 +63,12 @@ class UnevenBatch:
     def _s(stream):
         return (stream or torch.cuda.current_stream()).cuda_stream
 
+    def set_shapes(self, on=True):
+        """Relinearizations and rotations of every group with one persistent launch per
+        key-switch step (tb_uneven_set_shapes); set before capture()."""
+        self._lib.tb_uneven_set_shapes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        tb_capi.check(self._lib.tb_uneven_set_shapes(self.h, int(bool(on))))
+
     def run(self, stream=None):
         tb_capi.check(self._lib.tb_uneven_run(self.h, self._s(stream)))
 

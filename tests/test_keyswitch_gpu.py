@@ -205,3 +205,31 @@ def test_apply_galois_groups(orc, scheme, n, bits, t):
                                 _key_sub(keys[g], L))
             assert np.array_equal(got[b], exp), (g, b)
             b += 1
+
+
+@pytest.mark.parametrize("scheme,n,bits,t", [p for p in PARAMS if p[1] >= 4096])
+def test_persistent_keyswitch_matches_oracle(orc, scheme, n, bits, t):
+    """The persistent form (one launch per key-switch step, CTAs taking the next limb
+    from a device counter) gives the oracle's words too, for a relinearization and a
+    grouped multi-key rotation batch."""
+    moduli, t, ctx = _setup(orc, scheme, n, bits, t)
+    K = len(moduli)
+    logn = n.bit_length() - 1
+    rng = np.random.default_rng(n * 3 + scheme)
+    key = _rand(rng, moduli, n, (K - 1, 2))
+    lib = tb_capi.lib()
+    lib.tb_keyswitch_set_persistent(1)
+    try:
+        assert lib.tb_keyswitch_get_persistent() == 1
+        L = K - 1
+        B = 5
+        ct3 = _rand(rng, moduli[:L], n, (B, 3))
+        d = _dev(ct3)
+        ctx("relinearize", L, d, 0, _dev(key), B, None)
+        got = _host(d)
+        for b in (0, 2, B - 1):
+            exp = orc.keyswitch(scheme, logn, moduli, t, ct3[b, 2], ct3[b, :2], key)
+            assert np.array_equal(got[b, :2], exp), b
+    finally:
+        lib.tb_keyswitch_set_persistent(0)
+    assert lib.tb_keyswitch_get_persistent() == 0

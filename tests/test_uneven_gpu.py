@@ -60,11 +60,20 @@ def test_uneven_batch_graph_streams_per_op_and_reference_agree():
     streams = [g.out.clone() for g in groups]
     for g in groups:
         g.out.zero_()
+    # every group's key switches in one persistent launch per step
+    batch.set_shapes(True)
+    batch.run()
+    torch.cuda.synchronize()
+    for gi, g in enumerate(groups):
+        assert torch.equal(g.out, streams[gi]), gi
+        g.out.zero_()
+    batch.set_shapes(False)
     batch.run_per_op()
     torch.cuda.synchronize()
     per_op = [g.out.clone() for g in groups]
     for g in groups:
         g.out.zero_()
+    batch.set_shapes(True)
     batch.capture()
     batch.replay()
     batch.replay()  # twice: replays are repeatable
