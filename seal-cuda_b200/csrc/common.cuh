@@ -27,11 +27,14 @@ __device__ __forceinline__ uint64_t mul_shoup_lazy(uint64_t x, uint64_t w, uint6
 }
 
 __device__ __forceinline__ uint64_t mul_shoup(uint64_t x, uint64_t w, uint64_t wq, uint64_t q) {
-    uint64_t r = mul_shoup_lazy(x, w, wq, q);
-    return r >= q ? r - q : r;
+    const uint64_t r = mul_shoup_lazy(x, w, wq, q);
+    return min(r, r - q);
 }
 
-__device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t q) { return x >= q ? x - q : x; }
+// x mod q for x < 2q (any x < q + 2^63): x - q wraps above x exactly when x < q, so the
+// unsigned minimum picks the reduced value (a subtraction and a minimum, no compare
+// and select).
+__device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t q) { return min(x, x - q); }
 
 __device__ __forceinline__ uint64_t add_mod(uint64_t a, uint64_t b, uint64_t q) { return csub(a + b, q); }
 

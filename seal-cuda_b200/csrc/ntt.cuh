@@ -63,7 +63,7 @@ struct NttCfg {
 __host__ __device__ constexpr int swz_delta(int kk) { return kk ^ ((kk >> 4) & 15); }
 
 __device__ __forceinline__ void ct_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
-    uint64_t u = x >= q2 ? x - q2 : x;
+    uint64_t u = csub(x, q2);
     uint64_t v = mul_shoup_lazy(y, w.x, w.y, q);
     x = u + v;
     y = u + q2 - v;
@@ -72,7 +72,7 @@ __device__ __forceinline__ void ct_butterfly(uint64_t &x, uint64_t &y, ulonglong
 __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     uint64_t u = x, v = y;
     uint64_t s = u + v;
-    x = s >= q2 ? s - q2 : s;
+    x = csub(s, q2);
     y = mul_shoup_lazy(u + q2 - v, w.x, w.y, q);
 }
 
@@ -245,10 +245,10 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
                 for (int k = 0; k < R; k++) {
                     if (k & h) continue;
                     if (SCALE && t == R_LOG - 1) {
-                        uint64_t u = v[it][k] >= q2 ? v[it][k] - q2 : v[it][k];
+                        uint64_t u = csub(v[it][k], q2);
                         uint64_t y = v[it][k + h];
                         uint64_t sum = u + y;
-                        sum = sum >= q2 ? sum - q2 : sum;
+                        sum = csub(sum, q2);
                         v[it][k] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
                         v[it][k + h] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
                     } else {
@@ -384,9 +384,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THR
         for (int j = (int)half * (NB / 2) + threadIdx.x; j < (int)(half + 1) * (NB / 2); j += T) {
             const int p = swz(j);
             const uint64_t x = lo[p], y = hi[p];
-            const uint64_t u = x >= q2 ? x - q2 : x;
+            const uint64_t u = csub(x, q2);
             uint64_t sum = u + y;
-            sum = sum >= q2 ? sum - q2 : sum;
+            sum = csub(sum, q2);
             lo[p] = mul_shoup_lazy(sum, c.lm.inv_n, c.lm.inv_n_quo, q);
             hi[p] = mul_shoup_lazy(u + q2 - y, c.lm.sroot, c.lm.sroot_quo, q);
         }
@@ -430,9 +430,9 @@ __device__ __forceinline__ void cross_stage(uint64_t *xs, uint64_t *ys, int j0, 
             if constexpr (FWD) {
                 ct_butterfly(x[u], y[u], w, q, q2);
             } else if constexpr (SCALE) {
-                const uint64_t a = x[u] >= q2 ? x[u] - q2 : x[u];
+                const uint64_t a = csub(x[u], q2);
                 uint64_t sum = a + y[u];
-                sum = sum >= q2 ? sum - q2 : sum;
+                sum = csub(sum, q2);
                 const uint64_t dif = a + q2 - y[u];
                 x[u] = mul_shoup_lazy(sum, lm.inv_n, lm.inv_n_quo, q);
                 y[u] = mul_shoup_lazy(dif, lm.sroot, lm.sroot_quo, q);
