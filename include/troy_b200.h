@@ -263,6 +263,14 @@ int tb_encrypt_symmetric_seeded(tb_context *ctx, const uint64_t *seed8, const ui
  */
 int tb_expand_seeded(tb_context *ctx, int L, uint64_t seed, int inverse_ntt, uint64_t *c1, void *stream);
 /*
+ * tb_expand_seeded for `count` ciphertexts in one launch: seeds is a device array of
+ * count seeds (each non-zero), c1 of ciphertext b goes to c1 + b*c1_stride (0 = L*n).
+ * For a server that receives a batch of seed-compressed ciphertexts (c0 and the seed
+ * each, half the bytes of full ones); the reference loads them one per call.
+ */
+int tb_expand_seeded_batch(tb_context *ctx, int L, const uint64_t *seeds, uint64_t count, int inverse_ntt,
+                           uint64_t *c1, uint64_t c1_stride, void *stream);
+/*
  * Decrypts `batch` ciphertexts of `size` polynomials at level L (DecryptorCuda::decrypt,
  * src/decryptor_cuda.cu:92-328): BFV scale-and-round / BGV exact conversion (times
  * correction^-1) give n words mod t per plaintext; CKKS gives [L][n] in NTT form.

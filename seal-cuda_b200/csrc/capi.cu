@@ -43,6 +43,8 @@ int encrypt_symmetric(Context &c, const uint64_t *seed8, const uint64_t *sk, int
 int decrypt(Context &c, const uint64_t *sk, int L, int size, const uint64_t *ct, uint64_t cstride, uint64_t *out,
             uint64_t ostride, uint64_t correction, uint64_t B, cudaStream_t s);
 int expand_seeded(Context &c, int L, uint64_t seed, bool inverse_ntt, uint64_t *c1, cudaStream_t s);
+int expand_seeded_batch(Context &c, int L, const uint64_t *seeds, uint64_t count, bool inverse_ntt, uint64_t *c1,
+                        uint64_t stride, cudaStream_t s);
 int batch_encode(Context &c, const uint64_t *slots, uint64_t sstride, uint32_t count, uint64_t *out, uint64_t B,
                  cudaStream_t s);
 int batch_decode(Context &c, const uint64_t *plain, uint64_t *slots, uint64_t sstride, uint64_t B, cudaStream_t s);
@@ -310,6 +312,13 @@ int tb_encrypt_symmetric_seeded(tb_context *ctx, const uint64_t *seed8, const ui
         if (plain_count > c.n) return set_error(tb::TB_ERR_INVALID_ARGUMENT, "plaintext longer than the ring degree");
         return tb::encrypt_symmetric(c, seed8, sk, L, plain, plain_stride, (uint32_t)plain_count, ct, ct_stride, batch,
                                      S(stream), seeds);
+    });
+}
+
+int tb_expand_seeded_batch(tb_context *ctx, int L, const uint64_t *seeds, uint64_t count, int inverse_ntt,
+                           uint64_t *c1, uint64_t c1_stride, void *stream) {
+    return on_device(ctx, [&](tb::Context &c) {
+        return tb::expand_seeded_batch(c, L, seeds, count, inverse_ntt != 0, c1, c1_stride, S(stream));
     });
 }
 

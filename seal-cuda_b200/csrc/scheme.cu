@@ -615,6 +615,35 @@ __global__ void seeded_uniform_kernel(uint64_t *c1, const Mod *__restrict__ mods
     for (int j = 0; j < L; j++) c1[g + (size_t)j * n] = (uint64_t)(curand_uniform_double(&st) * (double)mods[j].value);
 }
 
+// The second polynomials of `count` seed-compressed ciphertexts at once: ciphertext b's
+// seed is seeds[b] (device memory), its c1 goes to c1 + b*stride; the same values as
+// expand_seeded per ciphertext.
+__global__ void seeded_uniform_batch_kernel(uint64_t *c1, uint64_t stride, const uint64_t *__restrict__ seeds,
+                                            const Mod *__restrict__ mods, int L, uint32_t n) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint64_t seed = seeds[blockIdx.y];
+    curandState st;
+    curand_init((unsigned long long)g + seed, 0ull, 0ull, &st);
+    uint64_t *out = c1 + (size_t)blockIdx.y * stride + g;
+    for (int j = 0; j < L; j++) out[(size_t)j * n] = (uint64_t)(curand_uniform_double(&st) * (double)mods[j].value);
+}
+
+int expand_seeded_batch(Context &c, int L, const uint64_t *seeds, uint64_t count, bool inverse_ntt, uint64_t *c1,
+                        uint64_t stride, cudaStream_t s) {
+    if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
+    if (!count) return TB_OK;
+    if (!c1 || !seeds) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (count > 65535) return set_error(TB_ERR_INVALID_ARGUMENT, "at most 65535 ciphertexts per call");
+    if (!stride) stride = (uint64_t)L * c.n;
+    dim3 grid((unsigned)((c.n + 255) / 256), (unsigned)count);
+    seeded_uniform_batch_kernel<<<grid, 256, 0, s>>>(c1, stride, seeds, c.d_mods, L, (uint32_t)c.n);
+    cudaError_t e = cudaGetLastError();
+    for (uint64_t b = 0; e == cudaSuccess && inverse_ntt && b < count; b++)
+        e = transform<false>(c, c1 + b * stride, 1, 0, L, false, s);
+    return status_from(e);
+}
+
 int expand_seeded(Context &c, int L, uint64_t seed, bool inverse_ntt, uint64_t *c1, cudaStream_t s) {
     if (L < 1 || L > (int)c.chain.size()) return set_error(TB_ERR_INVALID_ARGUMENT, "level outside the chain");
     if (!c1) return set_error(TB_ERR_INVALID_ARGUMENT, "null buffer");

@@ -181,3 +181,24 @@ def test_seeded_bgv_encryption_is_refused():
     plain = pytroy.BatchEncoder(ctx).encode(np.zeros(n, np.uint64))
     with pytest.raises(Exception, match="NTT domain"):
         encryptor.encrypt_symmetric_seeded(plain)
+
+
+@pytest.mark.parametrize("scheme,inverse", [(2, 0), (1, 1)])
+def test_batched_seed_expansion_equals_one_per_call(orc, scheme, inverse):
+    """tb_expand_seeded_batch writes, for every ciphertext of a batch, the second
+    polynomial tb_expand_seeded (the reference loader's cuRAND expansion) gives it."""
+    import tb_capi
+    n = 4096
+    moduli = orc.coeff_modulus_create(n, [36, 36, 37])
+    ctx = tb_capi.Context(scheme, n, moduli, 65537 if scheme == 1 else 0)
+    L, B = 2, 5
+    seeds = [0x1234567890abcdef + 977 * b for b in range(B)]
+    dseeds = torch.tensor(np.array(seeds, np.uint64).view(np.int64), device="cuda")
+    cts = torch.zeros((B, 2, L, n), dtype=torch.int64, device="cuda")
+    ctx("expand_seeded_batch", L, dseeds, B, inverse, cts[:, 1], 2 * L * n, None)
+    one = torch.zeros((L, n), dtype=torch.int64, device="cuda")
+    for b in range(B):
+        ctx("expand_seeded", L, seeds[b], inverse, one, None)
+        torch.cuda.synchronize()
+        assert torch.equal(cts[b, 1], one), b
+        assert not cts[b, 0].any()
