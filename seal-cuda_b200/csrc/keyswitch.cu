@@ -278,6 +278,61 @@ struct SpecialInttOp {
     }
 };
 
+// Steps 3 and 4 fused for the special prime: the inverse NTT whose load is the inner
+// product itself, acc = sum_j digit(b, j, special) * key[j][c][K-1] (lazy 128-bit sums,
+// one Barrett reduction), so the special-prime accumulator never goes through HBM;
+// output as SpecialInttOp (rounding offset for CKKS/BFV, canonical for BGV).
+struct SpecialInnerOp {
+    const uint64_t *digits;   // [B][L][L+1][N]
+    KeyGroups keys;
+    uint64_t *last;           // [B][2][N]
+    const Mod *mods;
+    int L, K, bgv, logn;
+    struct Ctx {
+        NttLimb lm;
+        const uint64_t *d, *k;
+        uint64_t *out;
+        uint64_t ratio_lo, ratio_hi;
+    };
+    __device__ Ctx ctx(int b) const {
+        const int cb = b >> 1, comp = b & 1;
+        const Mod &m = mods[K - 1];
+        Ctx c;
+        c.lm = make_limb(m, 0);
+        c.ratio_lo = m.ratio_lo;
+        c.ratio_hi = m.ratio_hi;
+        c.d = digits + (((size_t)cb * L * (L + 1) + L) << logn);
+        c.k = keys.of((uint32_t)cb) + (((size_t)comp * K + K - 1) << logn);
+        c.out = last + ((size_t)b << logn);
+        return c;
+    }
+    __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
+        const size_t dstep = (size_t)(L + 1) << logn, kstep = (size_t)(2 * K) << logn;
+        U128 s0{0, 0}, s1{0, 0};
+        const uint64_t *d = c.d + e, *k = c.k + e;
+        for (int j = 0; j < L; j++, d += dstep, k += kstep) {
+            const ulonglong2 dv = *reinterpret_cast<const ulonglong2 *>(d);
+            const ulonglong2 kv = __ldg(reinterpret_cast<const ulonglong2 *>(k));
+            mac128(s0, dv.x, kv.x);
+            mac128(s1, dv.y, kv.y);
+        }
+        Mod m;
+        m.value = c.lm.q;
+        m.ratio_lo = c.ratio_lo;
+        m.ratio_hi = c.ratio_hi;
+        a = reduce128(s0.hi, s0.lo, m);
+        b = reduce128(s1.hi, s1.lo, m);
+    }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const {
+        const uint64_t q = c.lm.q;
+        if (bgv) {
+            c.out[e] = csub(v, q);
+        } else {
+            c.out[e] = csub(csub(v + (q >> 1), 2 * q), q);
+        }
+    }
+};
+
 struct ModDownBase {
     const uint64_t *acc;      // [B][2][L+1][N]
     const uint64_t *last;     // [B][2][N]
@@ -451,16 +506,17 @@ int keyswitch_groups(const Context &c, int L, const uint64_t *target, uint64_t t
             e = dispatch_ntt<true>(logn, mu, (unsigned)(nb * pairs), 0, 0, s);
         }
         if (e != cudaSuccess) return status_from(e);
-        const int threads = 128;
-        dim3 grid((unsigned)((n / 2 + threads - 1) / threads), L + 1, (unsigned)nb);
+        // the data moduli's inner products; the special prime's runs inside its inverse NTT
+        const int threads = INNER_THREADS;
+        const KeyGroups kslice = keys.slice((uint32_t)b0, (uint32_t)nb);
+        dim3 grid((unsigned)((n / 2 + threads - 1) / threads), L, (unsigned)nb);
         {
             TraceScope ts("ks_inner_product", s);
-            ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, keys.slice((uint32_t)b0, (uint32_t)nb),
-                                                     acc, c.d_mods, L, K, ckks, logn);
+            ks_inner_kernel<<<grid, threads, 0, s>>>(digits, tg, tstride, kslice, acc, c.d_mods, L, K, ckks, logn);
             e = cudaGetLastError();
         }
         if (e != cudaSuccess) return status_from(e);
-        SpecialInttOp si{acc, last, c.d_mods, L, K, c.scheme == SCHEME_BGV, logn};
+        SpecialInnerOp si{digits, kslice, last, c.d_mods, L, K, c.scheme == SCHEME_BGV, logn};
         {
             TraceScope ts("ks_special_intt", s);
             e = dispatch_ntt<false>(logn, si, (unsigned)(nb * 2), logn, 1, s);
