@@ -132,7 +132,13 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
             for (int k = 0; k < R; k++) sm[sb ^ swz_delta(k << logsub)] = v[it][k];
         }
     }
-    __syncthreads();
+    // A radix-8 pass whose groups are 8 - 32 per block of 2^(LOGB-s) coefficients leaves
+    // each warp's 32 consecutive groups on 256 consecutive coefficients, exactly the ones
+    // the same warp's groups of the next radix-8 pass (s + 3) read: only the warp needs to
+    // wait there, so the warps of the CTA drift apart instead of meeting at a barrier.
+    constexpr int ls = LOGB - s - R_LOG;
+    if constexpr (R_LOG == 3 && ls >= 3 && ls <= 5 && T % 32 == 0) __syncwarp();
+    else __syncthreads();
 }
 
 // The radix-8 shared-memory passes from local stage S on, unrolled at compile time so
@@ -270,7 +276,13 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
             }
         }
     }
-    if constexpr (!TO_GLOBAL) __syncthreads();
+    // The first radix-8 pass (stages 0 - 2) leaves each warp's 32 consecutive groups on
+    // 256 consecutive coefficients, the ones the same warp's groups of the second
+    // radix-8 pass (stages 3 - 5) read: a warp barrier is enough between the two.
+    if constexpr (!TO_GLOBAL) {
+        if constexpr (R_LOG == 3 && s == 0 && LOGB >= 9 && T % 32 == 0) __syncwarp();
+        else __syncthreads();
+    }
 }
 
 // Radix-8 passes P .. PASSES-1 (local stages 3P ..), unrolled at compile time.
