@@ -76,6 +76,26 @@ __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong
     y = mul_shoup_lazy(u + q2 - v, w.x, w.y, q);
 }
 
+// Group handled by this thread in iteration i of a pass with IT groups per thread:
+// thread-major (i * T + thread) for a pass that loads from global memory (consecutive
+// threads take consecutive groups: coalesced), warp-major otherwise (warp w owns the
+// 32 IT consecutive groups from 32 IT w): a warp's groups then cover whole blocks of as
+// many stages as possible, so more of the barriers between passes can be warp barriers.
+// Within a warp the lanes still take consecutive groups, so shared-memory banks are hit
+// exactly as in the thread-major order.
+template <bool WARP_MAJOR, int T, int IT>
+__device__ __forceinline__ int pass_group(int i) {
+    if constexpr (WARP_MAJOR && IT > 1 && T % 32 == 0)
+        return (int)(threadIdx.x >> 5) * (32 * IT) + i * 32 + (int)(threadIdx.x & 31);
+    else
+        return (int)threadIdx.x + i * T;
+}
+
+template <int N>
+constexpr int ilog2c() {
+    return N <= 1 ? 0 : 1 + ilog2c<N / 2>();
+}
+
 // ---------------------------------------------------------------- forward
 // Pass of R_LOG Cooley-Tukey stages starting at local stage s. rbase = 2^s0 + sb
 // where s0 is the global stage of local stage 0 (0 when the CTA owns the limb).
@@ -97,7 +117,7 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
         uint64_t v[GR][R];
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<!FROM_GLOBAL, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const int base = ((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1));
             const int sb = swz(base);
@@ -109,7 +129,7 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
         }
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<!FROM_GLOBAL, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const uint32_t X = (rbase << s) + (uint32_t)(g >> logsub);
 #pragma unroll
@@ -125,19 +145,21 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
         }
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<!FROM_GLOBAL, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const int sb = swz(((g >> logsub) << (LOGB - s)) + (g & ((1 << logsub) - 1)));
 #pragma unroll
             for (int k = 0; k < R; k++) sm[sb ^ swz_delta(k << logsub)] = v[it][k];
         }
     }
-    // A radix-8 pass whose groups are 8 - 32 per block of 2^(LOGB-s) coefficients leaves
-    // each warp's 32 consecutive groups on 256 consecutive coefficients, exactly the ones
-    // the same warp's groups of the next radix-8 pass (s + 3) read: only the warp needs to
-    // wait there, so the warps of the CTA drift apart instead of meeting at a barrier.
+    // A shared-memory radix-8 pass with 2^ls groups per block of 2^(LOGB-s) coefficients,
+    // 8 <= 2^ls <= 32 IT, leaves each warp's 32 IT groups on 256 IT consecutive
+    // coefficients, exactly the ones the same warp's groups of the next radix-8 pass
+    // (s + 3) read: only the warp needs to wait there, so the warps of the CTA drift apart
+    // instead of meeting at a barrier.
     constexpr int ls = LOGB - s - R_LOG;
-    if constexpr (R_LOG == 3 && ls >= 3 && ls <= 5 && T % 32 == 0) __syncwarp();
+    constexpr int LIT = (IT > 1 && T % 32 == 0) ? ilog2c<IT>() : 0;
+    if constexpr (!FROM_GLOBAL && R_LOG == 3 && ls >= 3 && ls <= 5 + LIT && T % 32 == 0) __syncwarp();
     else __syncthreads();
 }
 
@@ -230,7 +252,7 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
         uint64_t v[GR][R];
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<true, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const int sb = swz(((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1)));
 #pragma unroll
@@ -238,7 +260,7 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
         }
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<true, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const int blk = g >> s;
 #pragma unroll
@@ -265,7 +287,7 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
         }
 #pragma unroll
         for (int it = 0; it < GR; it++) {
-            const int g = threadIdx.x + (i0 + it) * T;
+            const int g = pass_group<true, T, IT>(i0 + it);
             if (!FULL && g >= G) continue;
             const int base = ((g >> s) << (s + R_LOG)) + (g & ((1 << s) - 1));
             const int sb = swz(base);
@@ -276,11 +298,14 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
             }
         }
     }
-    // The first radix-8 pass (stages 0 - 2) leaves each warp's 32 consecutive groups on
-    // 256 consecutive coefficients, the ones the same warp's groups of the second
-    // radix-8 pass (stages 3 - 5) read: a warp barrier is enough between the two.
+    // A radix-8 pass at stage s with 2^(s+3) <= 32 IT leaves each warp's 32 IT groups on
+    // 256 IT consecutive coefficients, the ones the same warp's groups of the next
+    // radix-8 pass (s + 3) read: a warp barrier is enough between the two.
     if constexpr (!TO_GLOBAL) {
-        if constexpr (R_LOG == 3 && s == 0 && LOGB >= 9 && T % 32 == 0) __syncwarp();
+        constexpr int LIT = (IT > 1 && T % 32 == 0) ? ilog2c<IT>() : 0;
+        constexpr int PASSES_8 = (LOGB % 3) ? LOGB / 3 : LOGB / 3 - 1;   // radix-8 passes before the last
+        constexpr bool next_radix8 = s + 3 < 3 * PASSES_8;
+        if constexpr (R_LOG == 3 && next_radix8 && s + 3 <= 5 + LIT && T % 32 == 0) __syncwarp();
         else __syncthreads();
     }
 }
