@@ -186,8 +186,8 @@ struct PlainNttOp {
     __device__ uint64_t fix(const Ctx &c, uint64_t v) const {
         if (lazy) return v;
         const uint64_t q = c.lm.q;
-        if (FWD) v = v >= 2 * q ? v - 2 * q : v;
-        return v >= q ? v - q : v;
+        if (FWD) v = csub(v, 2 * q);
+        return csub(v, q);
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = fix(c, v); }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {

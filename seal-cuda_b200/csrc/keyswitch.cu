@@ -73,8 +73,7 @@ struct KsShape {
 namespace {
 
 __device__ __forceinline__ uint64_t full_fwd(uint64_t v, uint64_t q) {
-    v = v >= 2 * q ? v - 2 * q : v;
-    return v >= q ? v - q : v;
+    return csub(csub(v, 2 * q), q);
 }
 
 // [P][limbs] limbs at base + p*stride + l*N -> out + p*ostride + l*N.
@@ -106,7 +105,7 @@ struct StridedNttOp {
     }
     __device__ uint64_t fix(const Ctx &c, uint64_t v) const {
         if (lazy) return v;
-        return FWD ? full_fwd(v, c.lm.q) : (v >= c.lm.q ? v - c.lm.q : v);
+        return FWD ? full_fwd(v, c.lm.q) : csub(v, c.lm.q);
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = fix(c, v); }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {

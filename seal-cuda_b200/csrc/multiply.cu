@@ -430,7 +430,7 @@ struct CtInttOutOp {
         a = v.x;
         b = v.y;
     }
-    __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = v >= c.lm.q ? v - c.lm.q : v; }
+    __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = csub(v, c.lm.q); }
 };
 
 }  // namespace

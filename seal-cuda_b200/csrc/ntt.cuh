@@ -96,6 +96,24 @@ constexpr int ilog2c() {
     return N <= 1 ? 0 : 1 + ilog2c<N / 2>();
 }
 
+// Coefficient pairs moved between global and shared memory (forward copy-out, inverse
+// copy-in) in warp-major order when every thread has whole radix-8 groups (NB >= 8 T):
+// warp w moves coefficients w E .. (w+1) E - 1, E = 32 NB / T, 64 consecutive per
+// instruction (coalesced), exactly the coefficients its groups hold in the last forward
+// / first inverse radix-8 pass, so only a warp barrier separates the two.
+template <int NB, int T>
+struct WarpIO {
+    static constexpr bool value = T % 32 == 0 && NB % (8 * T) == 0;
+};
+
+template <int NB, int T>
+__device__ __forceinline__ int io_pair(int i) {
+    if constexpr (WarpIO<NB, T>::value)
+        return (int)(threadIdx.x >> 5) * (NB * 32 / T) + i * 64 + 2 * (int)(threadIdx.x & 31);
+    else
+        return (int)threadIdx.x * 2 + i * 2 * T;
+}
+
 // ---------------------------------------------------------------- forward
 // Pass of R_LOG Cooley-Tukey stages starting at local stage s. rbase = 2^s0 + sb
 // where s0 is the global stage of local stage 0 (0 when the CTA owns the limb).
@@ -157,9 +175,11 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
     // coefficients, exactly the ones the same warp's groups of the next radix-8 pass
     // (s + 3) read: only the warp needs to wait there, so the warps of the CTA drift apart
     // instead of meeting at a barrier.
+    // The last pass (ls = 0) hands each warp's coefficients to the same warp's copy-out.
     constexpr int ls = LOGB - s - R_LOG;
     constexpr int LIT = (IT > 1 && T % 32 == 0) ? ilog2c<IT>() : 0;
     if constexpr (!FROM_GLOBAL && R_LOG == 3 && ls >= 3 && ls <= 5 + LIT && T % 32 == 0) __syncwarp();
+    else if constexpr (!FROM_GLOBAL && R_LOG == 3 && ls == 0 && WarpIO<NB, T>::value) __syncwarp();
     else __syncthreads();
 }
 
@@ -186,21 +206,32 @@ struct HasEpi<Op, std::void_t<typename Op::Epi>> : std::true_type {};
 template <int NB, int T, class Op, class Ctx>
 __device__ __forceinline__ void fwd_copy_out(const Op &op, const Ctx &c, const uint64_t *sm, int off) {
     constexpr int ITER = NB / (2 * T);
-    if constexpr (HasEpi<Op>::value && ITER >= 1 && NB % (2 * T) == 0) {
+    if constexpr (WarpIO<NB, T>::value && !HasEpi<Op>::value) {
+#pragma unroll
+        for (int i = 0; i < ITER; i++) {
+            const int e = io_pair<NB, T>(i);
+            const int p = swz(e);
+            const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
+            // a select, not a branch: the slot parity changes every 8 lanes, and a branch
+            // would run both copies of the store (and its reductions) one after the other
+            const uint64_t a = (p & 1) ? w.y : w.x, b = (p & 1) ? w.x : w.y;
+            op.store2(c, e + off, a, b);
+        }
+    } else if constexpr (HasEpi<Op>::value && ITER >= 1 && NB % (2 * T) == 0) {
         constexpr int BATCH = ITER >= 4 ? 4 : ITER;
         static_assert(ITER % BATCH == 0, "copy-out batches");
 #pragma unroll
         for (int i0 = 0; i0 < ITER; i0 += BATCH) {
             typename Op::Epi pre[BATCH];
 #pragma unroll
-            for (int i = 0; i < BATCH; i++) pre[i] = op.epi2(c, threadIdx.x * 2 + (i0 + i) * 2 * T + off);
+            for (int i = 0; i < BATCH; i++) pre[i] = op.epi2(c, io_pair<NB, T>(i0 + i) + off);
 #pragma unroll
             for (int i = 0; i < BATCH; i++) {
-                const int e = threadIdx.x * 2 + (i0 + i) * 2 * T;
+                const int e = io_pair<NB, T>(i0 + i);
                 const int p = swz(e);
                 const ulonglong2 w = *reinterpret_cast<const ulonglong2 *>(&sm[p & ~1]);
-                if (p & 1) op.store2(c, e + off, w.y, w.x, pre[i]);
-                else op.store2(c, e + off, w.x, w.y, pre[i]);
+                const uint64_t a = (p & 1) ? w.y : w.x, b = (p & 1) ? w.x : w.y;
+                op.store2(c, e + off, a, b, pre[i]);
             }
         }
     } else {
@@ -319,6 +350,36 @@ __device__ __forceinline__ void inv_passes(const Op &op, const Ctx &c, uint64_t 
     }
 }
 
+// Copy-in of an inverse transform: coefficient pairs from op.load2 (coefficient e + off)
+// into shared memory, then the barrier before the first pass: a warp barrier when the
+// copy-in is warp-major and the first pass is a radix-8 pass (each warp then reads
+// exactly what it wrote), a CTA barrier otherwise.
+template <int LOGB, int T, class Op, class Ctx>
+__device__ __forceinline__ void inv_copy_in(const Op &op, const Ctx &c, uint64_t *sm, int off) {
+    constexpr int NB = 1 << LOGB;
+    constexpr int PASSES_8 = (LOGB % 3) ? LOGB / 3 : LOGB / 3 - 1;
+    if constexpr (WarpIO<NB, T>::value) {
+#pragma unroll 4
+        for (int i = 0; i < NB / (2 * T); i++) {
+            const int e = io_pair<NB, T>(i);
+            uint64_t a, b;
+            op.load2(c, e + off, a, b);
+            const int p = swz(e);
+            *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
+        }
+        if constexpr (PASSES_8 >= 1) __syncwarp();
+        else __syncthreads();
+    } else {
+        for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
+            uint64_t a, b;
+            op.load2(c, e + off, a, b);
+            const int p = swz(e);
+            *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
+        }
+        __syncthreads();
+    }
+}
+
 // One limb (or sub-block) b of Op by a CTA of T threads; scale_last: this CTA's last
 // stage is the transform's last stage (whole limb).
 template <int LOGB, int T, class Op>
@@ -326,16 +387,7 @@ __device__ __forceinline__ void ntt_inv_limb(const Op &op, int limb, int logn, i
     constexpr int NB = 1 << LOGB;
     constexpr int REM = LOGB % 3;
     const auto c = op.ctx(limb);
-    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
-        uint64_t a, b;
-        op.load2(c, e, a, b);
-        const int p = swz(e);
-        ulonglong2 w;
-        if (p & 1) w = make_ulonglong2(b, a);
-        else w = make_ulonglong2(a, b);
-        *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = w;
-    }
-    __syncthreads();
+    inv_copy_in<LOGB, T>(op, c, sm, 0);
     constexpr int LAST = REM ? REM : 3;
     constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;  // radix-8 passes before the last one
     inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, logn);
@@ -403,13 +455,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttCfg<LOGB, V>::THR
     auto c = op.ctx((int)(blockIdx.x >> 1));
     c.lm.sb = half;
     const int off = (int)half << LOGB;
-    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
-        uint64_t a, b;
-        op.load2(c, e + off, a, b);
-        const int p = swz(e);
-        *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
-    }
-    __syncthreads();
+    inv_copy_in<LOGB, T>(op, c, sm, off);
     constexpr int LAST = REM ? REM : 3;
     constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;
     inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, LOGB + 1);
@@ -531,13 +577,7 @@ __global__ void __cluster_dims__(1 << CLOG, 1, 1) __launch_bounds__(NttCfg<LOGB,
     auto c = op.ctx((int)(blockIdx.x >> CLOG));
     c.lm.sb = r;
     const int off = (int)r << LOGB;
-    for (int e = threadIdx.x * 2; e < NB; e += T * 2) {
-        uint64_t a, b;
-        op.load2(c, e + off, a, b);
-        const int p = swz(e);
-        *reinterpret_cast<ulonglong2 *>(&sm[p & ~1]) = (p & 1) ? make_ulonglong2(b, a) : make_ulonglong2(a, b);
-    }
-    __syncthreads();
+    inv_copy_in<LOGB, T>(op, c, sm, off);
     constexpr int LAST = REM ? REM : 3;
     constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;
     inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, LOGN);

@@ -82,7 +82,7 @@ struct LastInttOp {
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        v = v >= q ? v - q : v;           // canonical inverse transform
+        v = csub(v, q);                   // canonical inverse transform
         uint64_t x = v + (q >> 1);
         c.out[e] = x >= q ? x - q : x;
     }
