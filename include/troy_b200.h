@@ -415,6 +415,11 @@ int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_
    rate over this one is its fraction of the integer ceiling. No counterpart in the
    reference. */
 int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
+/* The same rate for the butterfly without the conditional subtraction of its first
+   input, which the key-switch mod-up transforms run for key moduli below 2^58 (their
+   consumer, the 128-bit inner product, takes the unreduced outputs). No counterpart in
+   the reference. */
+int tb_measure_slack_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
 /* Scratch budget of one key-switch launch sequence: a batch whose intermediates exceed
    it is processed in chunks (default 2 GiB, or the TB_KS_SCRATCH_BYTES environment
    value; 0 restores the default). */

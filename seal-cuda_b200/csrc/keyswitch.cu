@@ -125,13 +125,18 @@ struct ModUpOp {
     const Mod *mods;
     const uint64_t *chain;    // device copy of chain values (for the reduce test)
     int L, K, ckks, logn;
-    static constexpr int LAZY_MAX_L = 15;   // digits summed lazily from [0, 4q)
+    // Up to 15 digits are summed unreduced by the 128-bit inner products: from [0, 4q),
+    // or, for a key modulus below 2^58, straight from the slack transform (below
+    // (4 + 2 log2 N) q <= 38 q: 15 products of at most 38 q * q < 2^121.3 each stay
+    // below 2^128).
+    static constexpr int LAZY_MAX_L = 15;
     struct Ctx {
         NttLimb lm;
         const uint64_t *in;
         uint64_t *out;
         uint64_t ratio_hi;
         int reduce;
+        int slack;
     };
     __device__ Ctx ctx(int b) const {
         const int P = ckks ? L * L : L * (L + 1);
@@ -151,6 +156,7 @@ struct ModUpOp {
         c.lm = make_limb(m, 0);
         c.ratio_hi = m.ratio_hi;
         c.reduce = mods[j].value > m.value;
+        c.slack = L <= LAZY_MAX_L && m.value < (1ull << 58);
         c.in = src + (size_t)cb * sstride + ((size_t)j << logn);
         c.out = digits + ((((size_t)cb * L + j) * (L + 1) + i) << logn);
         return c;

@@ -69,6 +69,25 @@ __device__ __forceinline__ void ct_butterfly(uint64_t &x, uint64_t &y, ulonglong
     y = u + q2 - v;
 }
 
+// The Cooley-Tukey butterfly without the conditional subtraction of x: for a consumer
+// that reduces the transform's outputs itself. x grows by at most 2q a stage (y stays
+// below x's bound + 2q; the Shoup product is in [0, 2q) for any 64-bit input), so a
+// transform of S such stages from inputs below 4q ends below (4 + 2 S) q.
+__device__ __forceinline__ void ct_butterfly_slack(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
+    const uint64_t v = mul_shoup_lazy(y, w.x, w.y, q);
+    y = x + q2 - v;
+    x = x + v;
+}
+
+// An Op context with a member `slack` marks CTAs whose outputs may stay unreduced (see
+// ct_butterfly_slack); the single-CTA forward transform then runs the slack stages when
+// it is set. The Op guarantees (4 + 2 log2 N) q < 2^64 and that its consumer takes the
+// larger values.
+template <class Ctx, class = void>
+struct HasSlack : std::false_type {};
+template <class Ctx>
+struct HasSlack<Ctx, std::void_t<decltype(std::declval<Ctx>().slack)>> : std::true_type {};
+
 __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     uint64_t u = x, v = y;
     uint64_t s = u + v;
@@ -120,7 +139,7 @@ __device__ __forceinline__ int io_pair(int i) {
 // SIDE: the thread's groups are processed side by side (all loaded, then all
 // butterflies, then all stored: more independent work, more registers) rather than
 // one after another.
-template <int R_LOG, bool FROM_GLOBAL, int LOGB, int T, int s, bool SIDE, class Op, class Ctx>
+template <int R_LOG, bool FROM_GLOBAL, int LOGB, int T, int s, bool SIDE, bool SLACK = false, class Op, class Ctx>
 __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     constexpr int R = 1 << R_LOG;
     constexpr int NB = 1 << LOGB;
@@ -157,7 +176,8 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     if (k & half) continue;
-                    ct_butterfly(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
+                    if constexpr (SLACK) ct_butterfly_slack(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
+                    else ct_butterfly(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
                 }
             }
         }
@@ -185,11 +205,11 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 
 // The radix-8 shared-memory passes from local stage S on, unrolled at compile time so
 // every index offset is a constant.
-template <int S, int LOGB, int T, bool SIDE, class Op, class Ctx>
+template <int S, int LOGB, int T, bool SIDE, bool SLACK = false, class Op, class Ctx>
 __device__ __forceinline__ void fwd_passes(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     if constexpr (S < LOGB) {
-        fwd_pass<3, false, LOGB, T, S, SIDE>(op, c, sm, rbase);
-        fwd_passes<S + 3, LOGB, T, SIDE>(op, c, sm, rbase);
+        fwd_pass<3, false, LOGB, T, S, SIDE, SLACK>(op, c, sm, rbase);
+        fwd_passes<S + 3, LOGB, T, SIDE, SLACK>(op, c, sm, rbase);
     }
 }
 
@@ -246,16 +266,26 @@ __device__ __forceinline__ void fwd_copy_out(const Op &op, const Ctx &c, const u
 }
 
 // One limb (or sub-block) b of Op by a CTA of T threads, starting at global stage s0.
+template <bool SLACK, int LOGB, int T, class Op, class Ctx>
+__device__ __forceinline__ void ntt_fwd_block(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
+    constexpr int REM = LOGB % 3;
+    constexpr int FIRST = REM != 0 ? REM : 3;
+    fwd_pass<FIRST, true, LOGB, T, 0, false, SLACK>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, false, SLACK>(op, c, sm, rbase);
+    fwd_copy_out<1 << LOGB, T>(op, c, sm, 0);   // coalesced, two coefficients per thread
+}
+
 template <int LOGB, int T, class Op>
 __device__ __forceinline__ void ntt_fwd_limb(const Op &op, int limb, int s0, uint64_t *sm) {
-    constexpr int NB = 1 << LOGB;
-    constexpr int REM = LOGB % 3;
     const auto c = op.ctx(limb);
     const uint32_t rbase = (1u << s0) + c.lm.sb;
-    constexpr int FIRST = REM != 0 ? REM : 3;
-    fwd_pass<FIRST, true, LOGB, T, 0, false>(op, c, sm, rbase);
-    fwd_passes<FIRST, LOGB, T, false>(op, c, sm, rbase);
-    fwd_copy_out<NB, T>(op, c, sm, 0);   // coalesced, two coefficients per thread
+    if constexpr (HasSlack<decltype(c)>::value) {
+        if (c.slack) {
+            ntt_fwd_block<true, LOGB, T>(op, c, sm, rbase);
+            return;
+        }
+    }
+    ntt_fwd_block<false, LOGB, T>(op, c, sm, rbase);
 }
 
 template <int LOGB, int V, class Op>

@@ -233,3 +233,33 @@ def test_persistent_keyswitch_matches_oracle(orc, scheme, n, bits, t):
     finally:
         lib.tb_keyswitch_set_persistent(0)
     assert lib.tb_keyswitch_get_persistent() == 0
+
+
+@pytest.mark.parametrize("scheme", [CKKS, BFV])
+def test_keyswitch_slack_bounds(orc, scheme):
+    """The mod-up transforms of key moduli below 2^58 skip the butterflies' conditional
+    subtraction and hand the inner product values below (4 + 2 log2 N) q. Worst case of
+    that bound: N = 16384, 58-bit data primes (the largest that take the slack path)
+    with random residues (products near q^2), 15 digits (the most summed unreduced),
+    and 16 digits, where the digits are reduced before the sum; a 60-bit special prime
+    runs the usual butterfly in the same launch. Bit-exact against the oracle."""
+    n = 16384
+    logn = n.bit_length() - 1
+    moduli = orc.coeff_modulus_create(n, [58] * 16 + [60])
+    assert all(q < (1 << 58) for q in moduli[:-1]) and moduli[-1] >= (1 << 58)
+    t = 0 if scheme == CKKS else orc.plain_modulus_batching(n, 20)
+    ctx = tb_capi.Context(scheme, n, moduli, t)
+    K = len(moduli)
+    rng = np.random.default_rng(58)
+    key = rng.integers(0, 1, (K - 1, 2, K, n), dtype=np.uint64)
+    for j, q in enumerate(moduli):
+        key[:, :, j] = rng.integers(q - (q >> 4), q, (K - 1, 2, n), dtype=np.uint64)
+    dkey = _dev(key)
+    for L in (15, 16):
+        data = moduli[:L]
+        target = np.stack([rng.integers(q - (q >> 4), q, n, dtype=np.uint64) for q in data])[None]
+        ct = _rand(rng, data, n, (1, 2))
+        dct = _dev(ct)
+        ctx("keyswitch", L, _dev(target), 0, dct, 0, dkey, 1, None)
+        exp = orc.keyswitch(scheme, logn, data + [moduli[-1]], t, target[0], ct[0], _key_sub(key, L))
+        assert np.array_equal(_host(dct)[0], exp), L

@@ -181,11 +181,16 @@ def test_raw_ntt_dyadic_sweep_configuration(orc, logn):
 
 
 def test_integer_ceiling_is_measured():
-    """The butterfly-rate microbenchmark runs and reports a plausible rate (between
-    1e10 and 1e14 butterflies per second on one GPU)."""
+    """The butterfly-rate microbenchmarks run and report plausible rates (between 1e10
+    and 1e14 butterflies per second on one GPU); the butterfly without the conditional
+    subtraction is not slower than the one with it."""
     import ctypes
     lib = tb_capi.lib()
-    lib.tb_measure_butterfly_rate.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
-    r = ctypes.c_double(0)
-    tb_capi.check(lib.tb_measure_butterfly_rate((1 << 60) - 93, None, ctypes.byref(r)))
-    assert 1e10 < r.value < 1e14
+    rates = []
+    for fn in (lib.tb_measure_butterfly_rate, lib.tb_measure_slack_butterfly_rate):
+        fn.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        r = ctypes.c_double(0)
+        tb_capi.check(fn((1 << 60) - 93, None, ctypes.byref(r)))
+        assert 1e10 < r.value < 1e14
+        rates.append(r.value)
+    assert rates[1] > 0.95 * rates[0]
