@@ -414,7 +414,7 @@ def run_b200(args, rank, world):
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH,
             "int_ceiling": int_ceiling(lib, moduli[0]), "int_ceiling_slack": int_ceiling(lib, moduli[0], slack=True),
-            "slack_share": modup_slack_share(moduli, L), "sub": SUB}
+            "slack_share": slack_shares(moduli, L, N.bit_length() - 1), "sub": SUB}
 
 
 def run_ntt_sweep(batch=256, reps=10):
@@ -423,7 +423,9 @@ def run_ntt_sweep(batch=256, reps=10):
     Algorithmic bytes: 16 N B L per transform (read + write), 24 N B L per dyadic
     product; GB/s and the fraction of the measured copy peak per kernel, and for the
     transforms the fraction of the integer ceiling ((N/2) log2 N butterflies per limb
-    over tb_measure_butterfly_rate)."""
+    over tb_measure_butterfly_rate; the forward transform (full outputs, deferred
+    reductions) over that rate and tb_measure_slack_butterfly_rate weighted by the
+    shares of its stages that run each butterfly)."""
     import torch
     import tb_capi
 
@@ -443,6 +445,10 @@ def run_ntt_sweep(batch=256, reps=10):
         moduli = [int(m) for m in mods]
         if ceiling is None:
             ceiling = int_ceiling(lib, moduli[0])
+            ceiling_slack = int_ceiling(lib, moduli[0], slack=True)
+        # forward: stages above 2^14 run separately (Harvey), the 2^14 blocks defer
+        sh = (min(logn, 14) - fwd_subtracting_stages(min(logn, 14))) / logn
+        ceilings = {"ntt_forward": 1.0 / (sh / ceiling_slack + (1.0 - sh) / ceiling), "ntt_inverse": ceiling}
         ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
         x = _rand_residues(torch, (batch, 8, n), moduli, gen)
         y = _rand_residues(torch, (batch, 8, n), moduli, gen)
@@ -478,7 +484,7 @@ def run_ntt_sweep(batch=256, reps=10):
             row[name] = {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4)}
             if name != "dyadic":   # against the integer ceiling: (N/2) log2 N butterflies per limb
                 rate = batch * 8 * (n // 2) * logn / (ms * 1e-3)
-                row[name]["frac_of_int_ceiling"] = round(rate / ceiling, 4)
+                row[name]["frac_of_int_ceiling"] = round(rate / ceilings[name], 4)
         row["variants"] = {"forward": vf.value, "inverse": vi.value}
         out[f"N={n}"] = row
         for fwd, v in zip((1, 0), saved):
@@ -486,7 +492,8 @@ def run_ntt_sweep(batch=256, reps=10):
         del x, y, z
         ctx.close()
     return {"workload": f"{batch} polynomials x 8 limbs (50-bit primes)",
-            "int_ceiling_gbutterflies_per_s": round(ceiling / 1e9, 2), "results": out}
+            "int_ceiling_gbutterflies_per_s": round(ceiling / 1e9, 2),
+            "int_ceiling_slack_gbutterflies_per_s": round(ceiling_slack / 1e9, 2), "results": out}
 
 
 UNEVEN_SHAPES = [(1, 4096, [36, 36, 37]), (3, 8192, [43, 43, 44, 44, 44]), (1, 16384, [48] * 9)]
@@ -728,10 +735,10 @@ def roofline(res, steps):
     if ceil_std:
         ceilings = {k: ceil_std for k in bfly}
         if res.get("int_ceiling_slack"):
-            # the mod-up runs the slack butterfly on the limbs of key moduli below 2^58:
-            # its ceiling is the two rates weighted by their share of its butterflies
-            sh = res["slack_share"]
-            ceilings["ks_modup_ntt"] = 1.0 / (sh / res["int_ceiling_slack"] + (1.0 - sh) / ceil_std)
+            # the forward transforms run the slack butterfly at most of their stages: their
+            # ceiling is the two rates weighted by their shares of the butterflies
+            for k, sh in res["slack_share"].items():
+                ceilings[k] = 1.0 / (sh / res["int_ceiling_slack"] + (1.0 - sh) / ceil_std)
     for k, row in table.items():
         if k in bfly and k in ceilings:
             rate = bfly[k] / (row["ms_per_step"] * 1e-3)
@@ -761,12 +768,12 @@ def roofline(res, steps):
         out["int"] = {"achieved": round(rate / 1e9, 2), "peak": round(ceil / 1e9, 2), "unit": "Gbutterfly/s",
                       "frac": round(rate / ceil, 4), "butterflies_per_launch": round(bfly[name] * steps / launches),
                       "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
-        if name == "ks_modup_ntt" and res.get("int_ceiling_slack"):
+        if name in res.get("slack_share", {}) and res.get("int_ceiling_slack"):
             out["int"]["peak_source"] = (
                 "measured here, operands in registers: tb_measure_butterfly_rate "
                 f"({ceil_std / 1e9:.2f} G/s) and tb_measure_slack_butterfly_rate "
-                f"({res['int_ceiling_slack'] / 1e9:.2f} G/s), weighted by the share of the mod-up's limbs "
-                f"on key moduli below 2^58 ({res['slack_share']:.4f}), which run the slack butterfly")
+                f"({res['int_ceiling_slack'] / 1e9:.2f} G/s), weighted by the share of the forward "
+                f"transform's butterflies that skip the subtraction ({res['slack_share'][name]:.4f})")
     return out
 
 
@@ -792,21 +799,40 @@ def int_ceiling(lib, q, slack=False):
     return r.value
 
 
-def modup_slack_share(moduli, L):
-    """Share of the mod-up transforms (CKKS: digit j onto every key modulus but its own,
-    at L data limbs and at L-1 after the rescale) whose key modulus is below 2^58: those
-    run the slack butterfly."""
+def fwd_subtracting_stages(logn, M=16):
+    """Stages of a forward transform of 2^logn coefficients with deferred reductions
+    (bound M q; the library's fwd_bound / fwd_subtracts) that run the subtracting
+    butterfly; the others run the slack one."""
+    b, sub = 4, 0
+    for _ in range(logn):
+        if b + 2 <= M:
+            b += 2
+        else:
+            b, sub = M // 2 + 2, sub + 1
+    return sub
+
+
+def slack_shares(moduli, L, logn):
+    """Per forward-transform kernel at the benchmark shape, the share of its butterflies
+    that run the slack butterfly (no subtraction). A limb of modulus q runs none of its
+    stages subtracting when q < 2^58 (in the key-switch mod-up: with at most 15 digits),
+    all but fwd_subtracting_stages(logn) of them when q < 2^60, every one otherwise. The
+    mod-up covers digit j on every key modulus but its own at L data limbs and at L-1
+    after the rescale; the mod-down and the rescale transform data limbs."""
     special = moduli[-1]
-    slack = total = 0
+    part = (logn - fwd_subtracting_stages(logn)) / logn
+
+    def share(q, wide):
+        return 1.0 if wide and q < (1 << 58) else part if q < (1 << 60) else 0.0
+
+    up = []
     for lv in (L, L - 1):
         targets = list(moduli[:lv]) + [special]
-        for j in range(lv):
-            for i, q in enumerate(targets):
-                if i == j:
-                    continue
-                total += 1
-                slack += q < (1 << 58) and lv <= 15
-    return slack / total
+        up += [share(q, lv <= 15) for j in range(lv) for i, q in enumerate(targets) if i != j]
+    down = [share(q, True) for lv in (L, L - 1) for q in moduli[:lv]]
+    resc = [share(q, True) for q in moduli[:L - 1]]
+    return {"ks_modup_ntt": sum(up) / len(up), "ks_moddown": sum(down) / len(down),
+            "rescale_ntt": sum(resc) / len(resc)}
 
 
 TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "ckks_step_n16384_traffic.md")

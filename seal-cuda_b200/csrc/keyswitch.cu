@@ -76,6 +76,11 @@ __device__ __forceinline__ uint64_t full_fwd(uint64_t v, uint64_t q) {
     return csub(csub(v, 2 * q), q);
 }
 
+// [0, q) from any value below 16 q (a forward transform with deferred reductions)
+__device__ __forceinline__ uint64_t full_fwd16(uint64_t v, uint64_t q) {
+    return full_fwd(csub(csub(v, 8 * q), 4 * q), q);
+}
+
 // [P][limbs] limbs at base + p*stride + l*N -> out + p*ostride + l*N.
 template <bool FWD>
 struct StridedNttOp {
@@ -125,11 +130,13 @@ struct ModUpOp {
     const Mod *mods;
     const uint64_t *chain;    // device copy of chain values (for the reduce test)
     int L, K, ckks, logn;
-    // Up to 15 digits are summed unreduced by the 128-bit inner products: from [0, 4q),
-    // or, for a key modulus below 2^58, straight from the slack transform (below
-    // (4 + 2 log2 N) q <= 38 q: 15 products of at most 38 q * q < 2^121.3 each stay
-    // below 2^128).
+    // Up to 15 digits are summed unreduced by the 128-bit inner products: below 4q (a
+    // 61-bit q), below 16 q (q < 2^60, deferred reductions) or below 38 q (q < 2^58, no
+    // subtraction at all): 15 products below 4 q * q < 2^124, 16 q * q < 2^124 or
+    // 38 q * q < 2^121.3 each stay below 2^128. More digits are reduced to [0, q) at the
+    // store (the transform then stays below 16 q).
     static constexpr int LAZY_MAX_L = 15;
+    static constexpr bool wide_slack = true;
     struct Ctx {
         NttLimb lm;
         const uint64_t *in;
@@ -156,7 +163,7 @@ struct ModUpOp {
         c.lm = make_limb(m, 0);
         c.ratio_hi = m.ratio_hi;
         c.reduce = mods[j].value > m.value;
-        c.slack = L <= LAZY_MAX_L && m.value < (1ull << 58);
+        c.slack = (L <= LAZY_MAX_L && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         c.in = src + (size_t)cb * sstride + ((size_t)j << logn);
         c.out = digits + ((((size_t)cb * L + j) * (L + 1) + i) << logn);
         return c;
@@ -168,8 +175,8 @@ struct ModUpOp {
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
         if (L > LAZY_MAX_L) {
-            a = full_fwd(a, c.lm.q);
-            b = full_fwd(b, c.lm.q);
+            a = full_fwd16(a, c.lm.q);
+            b = full_fwd16(b, c.lm.q);
         }
         *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(a, b);
     }
@@ -354,7 +361,9 @@ struct ModDownBase {
         uint64_t ratio_hi;
         DropC d;
         int reduce;
+        int slack;   // forward transform (CKKS) with deferred reductions: outputs below 16 q or 38 q
     };
+    static constexpr bool wide_slack = true;
     __device__ Ctx make(int b) const {
         const int j = b % L, bc = b / L;  // bc = cb*2 + c
         const int cb = bc >> 1, cc = bc & 1;
@@ -364,6 +373,7 @@ struct ModDownBase {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)K * K + j];
         c.reduce = mods[K - 1].value > m.value;
+        c.slack = m.value < (1ull << 58) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         c.acc = acc + (((size_t)bc * (L + 1) + j) << logn);
         c.last = last + ((size_t)bc << logn);
         c.ct = ct + (size_t)cb * cstride + (((size_t)cc * L + j) << logn);
@@ -382,6 +392,10 @@ struct ModDownBase {
 };
 
 // Step 5, CKKS: NTT of (r mod q_j) + fix, epilogue ct += (acc + 4 q_j - ntt) * q_k^-1.
+// After a transform with deferred reductions (ntt below 16 q_j, or 38 q_j for q_j <
+// 2^58) one subtraction of 8 q_j (32 q_j) brings ntt below 8 q_j (32 q_j) and the
+// epilogue takes acc + 8 q_j - ntt (acc + 32 q_j - ntt): below 9 q_j (33 q_j) < 2^64,
+// where acc + 16 q_j - ntt would pass 2^64 for a 60-bit q_j. The same residue each way.
 // The transform's input only has to stay below 4 q_j: a lazy residue (< 2 q_j) plus fix.
 struct ModDownCkksOp : ModDownBase {
     __device__ Ctx ctx(int b) const { return make(b); }
@@ -395,7 +409,9 @@ struct ModDownCkksOp : ModDownBase {
     }
     __device__ uint64_t fin(const Ctx &c, uint64_t acc, uint64_t ct, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        return add_mod(mul_shoup(acc + 4 * q - v, c.d.inv, c.d.inv_quo, q), ct, q);
+        const int sh = c.slack == SLACK_WIDE ? 5 : c.slack ? 3 : 2;
+        const uint64_t x = acc + (q << sh) - (c.slack ? csub(v, q << sh) : v);
+        return add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), ct, q);
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {
         *reinterpret_cast<ulonglong2 *>(c.ct + e) = make_ulonglong2(fin(c, p.acc.x, p.ct.x, a), fin(c, p.acc.y, p.ct.y, b));

@@ -69,24 +69,58 @@ __device__ __forceinline__ void ct_butterfly(uint64_t &x, uint64_t &y, ulonglong
     y = u + q2 - v;
 }
 
-// The Cooley-Tukey butterfly without the conditional subtraction of x: for a consumer
-// that reduces the transform's outputs itself. x grows by at most 2q a stage (y stays
-// below x's bound + 2q; the Shoup product is in [0, 2q) for any 64-bit input), so a
-// transform of S such stages from inputs below 4q ends below (4 + 2 S) q.
+// The Cooley-Tukey butterfly without the conditional subtraction of x, and the one that
+// subtracts a given multiple qs of q instead of 2q. Without the subtraction x grows by at
+// most 2q a stage (y stays below x's bound + 2q; the Shoup product is in [0, 2q) for any
+// 64-bit input).
 __device__ __forceinline__ void ct_butterfly_slack(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     const uint64_t v = mul_shoup_lazy(y, w.x, w.y, q);
     y = x + q2 - v;
     x = x + v;
 }
 
-// An Op context with a member `slack` marks CTAs whose outputs may stay unreduced (see
-// ct_butterfly_slack); the single-CTA forward transform then runs the slack stages when
-// it is set. The Op guarantees (4 + 2 log2 N) q < 2^64 and that its consumer takes the
-// larger values.
+__device__ __forceinline__ void ct_butterfly_sub(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2,
+                                                 uint64_t qs) {
+    const uint64_t u = csub(x, qs);
+    const uint64_t v = mul_shoup_lazy(y, w.x, w.y, q);
+    x = u + v;
+    y = u + q2 - v;
+}
+
+// Forward stages with deferred reductions, bound M (in multiples of q). Values entering
+// local stage k of a transform from inputs below 4q stay below fwd_bound(M, k) q: a stage
+// skips the subtraction (bound + 2q) unless that would pass M q; then it first subtracts
+// (M/2) q from x (x below (M/2) q, outputs below (M/2 + 2) q). M = 4 is the Harvey
+// butterfly of every stage (subtract 2q; outputs below 4q, the reference's lazy
+// outputs). M = 16, for q < 2^60 (16 q < 2^64), subtracts at two of the 14 stages of a
+// 16384-coefficient transform; its outputs stay below 16 q.
+__host__ __device__ constexpr int fwd_bound(int M, int k) {
+    int b = 4;
+    for (int i = 0; i < k; i++) b = b + 2 <= M ? b + 2 : M / 2 + 2;
+    return b;
+}
+__host__ __device__ constexpr bool fwd_subtracts(int M, int k) { return fwd_bound(M, k) + 2 > M; }
+static_assert(fwd_bound(4, 14) == 4 && fwd_subtracts(4, 0) && fwd_subtracts(4, 13), "Harvey stages");
+static_assert(fwd_bound(16, 17) <= 16 && !fwd_subtracts(16, 5) && fwd_subtracts(16, 6) && fwd_subtracts(16, 10),
+              "deferred stages");
+static_assert(fwd_bound(64, 17) == 38 && !fwd_subtracts(64, 16), "no subtraction below 2^58");
+
+// An Op context with an int member `slack` selects per CTA the bound M of its forward
+// transform: 0 for the Harvey stages, SLACK_M (q < 2^60: outputs below 16 q) or, for an
+// Op that declares `static constexpr bool wide_slack = true`, SLACK_WIDE (q < 2^58: no
+// subtraction at all, outputs below (4 + 2 log2 N) q <= 38 q). The Op takes those
+// outputs at its store. The CTA-pair and cluster forms always run the Harvey stages
+// (outputs below 4q).
+constexpr int SLACK_M = 16;
+constexpr int SLACK_WIDE = 64;
 template <class Ctx, class = void>
 struct HasSlack : std::false_type {};
 template <class Ctx>
 struct HasSlack<Ctx, std::void_t<decltype(std::declval<Ctx>().slack)>> : std::true_type {};
+template <class Op, class = void>
+struct WideSlack : std::false_type {};
+template <class Op>
+struct WideSlack<Op, std::void_t<decltype(Op::wide_slack)>> : std::bool_constant<Op::wide_slack> {};
 
 __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     uint64_t u = x, v = y;
@@ -139,7 +173,7 @@ __device__ __forceinline__ int io_pair(int i) {
 // SIDE: the thread's groups are processed side by side (all loaded, then all
 // butterflies, then all stored: more independent work, more registers) rather than
 // one after another.
-template <int R_LOG, bool FROM_GLOBAL, int LOGB, int T, int s, bool SIDE, bool SLACK = false, class Op, class Ctx>
+template <int R_LOG, bool FROM_GLOBAL, int LOGB, int T, int s, bool SIDE, int M = 4, class Op, class Ctx>
 __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     constexpr int R = 1 << R_LOG;
     constexpr int NB = 1 << LOGB;
@@ -148,7 +182,7 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
     constexpr int GR = SIDE ? IT : 1;                // groups in flight at once
     constexpr bool FULL = G > 0 && G % T == 0;
     constexpr int logsub = LOGB - s - R_LOG;
-    const uint64_t q = c.lm.q, q2 = q << 1;
+    const uint64_t q = c.lm.q, q2 = q << 1, qs = q * (uint64_t)(M / 2);
 #pragma unroll
     for (int i0 = 0; i0 < IT; i0 += GR) {
         uint64_t v[GR][R];
@@ -176,8 +210,10 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     if (k & half) continue;
-                    if constexpr (SLACK) ct_butterfly_slack(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
-                    else ct_butterfly(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
+                    if (fwd_subtracts(M, s + t))
+                        ct_butterfly_sub(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2, qs);
+                    else
+                        ct_butterfly_slack(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);
                 }
             }
         }
@@ -205,11 +241,11 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 
 // The radix-8 shared-memory passes from local stage S on, unrolled at compile time so
 // every index offset is a constant.
-template <int S, int LOGB, int T, bool SIDE, bool SLACK = false, class Op, class Ctx>
+template <int S, int LOGB, int T, bool SIDE, int M = 4, class Op, class Ctx>
 __device__ __forceinline__ void fwd_passes(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     if constexpr (S < LOGB) {
-        fwd_pass<3, false, LOGB, T, S, SIDE, SLACK>(op, c, sm, rbase);
-        fwd_passes<S + 3, LOGB, T, SIDE, SLACK>(op, c, sm, rbase);
+        fwd_pass<3, false, LOGB, T, S, SIDE, M>(op, c, sm, rbase);
+        fwd_passes<S + 3, LOGB, T, SIDE, M>(op, c, sm, rbase);
     }
 }
 
@@ -266,12 +302,12 @@ __device__ __forceinline__ void fwd_copy_out(const Op &op, const Ctx &c, const u
 }
 
 // One limb (or sub-block) b of Op by a CTA of T threads, starting at global stage s0.
-template <bool SLACK, int LOGB, int T, class Op, class Ctx>
+template <int M, int LOGB, int T, class Op, class Ctx>
 __device__ __forceinline__ void ntt_fwd_block(const Op &op, const Ctx &c, uint64_t *sm, uint32_t rbase) {
     constexpr int REM = LOGB % 3;
     constexpr int FIRST = REM != 0 ? REM : 3;
-    fwd_pass<FIRST, true, LOGB, T, 0, false, SLACK>(op, c, sm, rbase);
-    fwd_passes<FIRST, LOGB, T, false, SLACK>(op, c, sm, rbase);
+    fwd_pass<FIRST, true, LOGB, T, 0, false, M>(op, c, sm, rbase);
+    fwd_passes<FIRST, LOGB, T, false, M>(op, c, sm, rbase);
     fwd_copy_out<1 << LOGB, T>(op, c, sm, 0);   // coalesced, two coefficients per thread
 }
 
@@ -280,12 +316,18 @@ __device__ __forceinline__ void ntt_fwd_limb(const Op &op, int limb, int s0, uin
     const auto c = op.ctx(limb);
     const uint32_t rbase = (1u << s0) + c.lm.sb;
     if constexpr (HasSlack<decltype(c)>::value) {
+        if constexpr (WideSlack<Op>::value) {
+            if (c.slack == SLACK_WIDE) {
+                ntt_fwd_block<SLACK_WIDE, LOGB, T>(op, c, sm, rbase);
+                return;
+            }
+        }
         if (c.slack) {
-            ntt_fwd_block<true, LOGB, T>(op, c, sm, rbase);
+            ntt_fwd_block<SLACK_M, LOGB, T>(op, c, sm, rbase);
             return;
         }
     }
-    ntt_fwd_block<false, LOGB, T>(op, c, sm, rbase);
+    ntt_fwd_block<4, LOGB, T>(op, c, sm, rbase);
 }
 
 template <int LOGB, int V, class Op>

@@ -106,7 +106,9 @@ struct RescaleNttOp {
         uint64_t ratio_hi;
         DropC d;
         int reduce;
+        int slack;   // forward transform with deferred reductions: outputs below 16 q or 38 q
     };
+    static constexpr bool wide_slack = true;
     __device__ Ctx ctx(int b) const {
         const int j = b % (L - 1), p = b / (L - 1);
         const Mod &m = mods[j];
@@ -115,6 +117,7 @@ struct RescaleNttOp {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)L * K + j];
         c.reduce = mods[L - 1].value > m.value;
+        c.slack = m.value < (1ull << 58) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         const size_t cb = p / size, k = p % size;
         c.in = in + cb * istride + ((k * L + j) << logn);
         c.out = out + cb * ostride + ((k * (L - 1) + j) << logn);
@@ -134,7 +137,12 @@ struct RescaleNttOp {
     __device__ Epi epi2(const Ctx &c, int e) const { return {*reinterpret_cast<const ulonglong2 *>(c.in + e)}; }
     __device__ uint64_t fin(const Ctx &c, uint64_t in, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        return mul_shoup(in + 4 * q - v, c.d.inv, c.d.inv_quo, q);
+        // after deferred reductions v is below 16 q (38 q for q < 2^58): one subtraction
+        // of 8 q (32 q) keeps in + 8 q - v (in + 32 q - v) below 9 q (33 q) < 2^64
+        // (in + 16 q - v would pass 2^64 for a 60-bit q)
+        const int sh = c.slack == SLACK_WIDE ? 5 : c.slack ? 3 : 2;
+        const uint64_t x = in + (q << sh) - (c.slack ? csub(v, q << sh) : v);
+        return mul_shoup(x, c.d.inv, c.d.inv_quo, q);
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {
         *reinterpret_cast<ulonglong2 *>(c.out + e) = make_ulonglong2(fin(c, p.in.x, a), fin(c, p.in.y, b));

@@ -46,6 +46,52 @@ def test_ntt_roundtrip_all_sizes(orc, logn):
     assert torch.equal(y, d)
 
 
+def _is_prime(q):
+    """Deterministic Miller-Rabin for 64-bit q."""
+    if q < 2 or q % 2 == 0:
+        return q == 2
+    d, r = q - 1, 0
+    while d % 2 == 0:
+        d, r = d // 2, r + 1
+    for a in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+        x = pow(a, d, q)
+        if x in (1, q - 1):
+            continue
+        for _ in range(r - 1):
+            x = x * x % q
+            if x == q - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def _ntt_prime(bits, m):
+    """The largest prime below 2^bits that is 1 mod m."""
+    q = ((1 << bits) - 1) // m * m + 1
+    while not _is_prime(q):
+        q -= m
+    return q
+
+
+@pytest.mark.parametrize("logn", [12, 14, 15, 17])
+def test_ntt_full_forward_deferred_bounds(orc, logn):
+    """Full forward outputs of primes just below 2^60 (the largest whose transforms
+    defer their reductions to a bound of 16 q) and of a 61-bit prime (Harvey stages
+    throughout), from inputs anywhere in [0, 4q): bit-exact against the oracle."""
+    n = 1 << logn
+    moduli = orc.coeff_modulus_create(n, [60, 60]) + [_ntt_prime(61, 2 * n)]
+    assert moduli[0] >= (1 << 59) and moduli[-1] >= (1 << 60)
+    ctx = tb_capi.Context(tb_capi.SCHEME_RAW, n, moduli)
+    rng = np.random.default_rng(logn + 60)
+    x = np.stack([rng.integers(4 * q - (q >> 3), 4 * q, n, dtype=np.uint64) for q in moduli])
+    x[:, ::7] = np.asarray(moduli, np.uint64)[:, None] * 4 - 1
+    d = _dev(x)
+    out = torch.empty_like(d)
+    ctx("ntt_forward", d, out, 1, 0, len(moduli), 0, None)
+    assert np.array_equal(_host(out), orc.ntt_forward_rns(logn, moduli, x, lazy=False))
+
+
 def test_ntt_lazy_input_range(orc):
     """Forward accepts [0, 4q) inputs and inverse [0, 2q) inputs, as the reference."""
     logn, n = 12, 4096
