@@ -689,8 +689,11 @@ def algorithmic_bytes_per_step(L):
         return {
             "ks_target_intt": 2 * l * n * W,
             "ks_modup_ntt": (l + l * l) * n * W,                     # each target limb in once, L*L digits out
-            "ks_inner_product": (l * l + l + 2 * (l + 1)) * n * W,   # digits + target in, accumulators out
-            "ks_special_intt": 2 * 2 * n * W,
+            # digits of the l data moduli (l - 1 per modulus) + the target limb in,
+            # 2 l accumulators out
+            "ks_inner_product": (l * l + 2 * l) * n * W,
+            # the l special-modulus digits in (inner product fused into the load), 2 rows out
+            "ks_special_intt": (l + 2) * n * W,
             "ks_moddown": 2 * l * 4 * n * W,                         # last, acc, ct in; ct out
         }
 
@@ -702,8 +705,10 @@ def algorithmic_bytes_per_step(L):
         out[name] = B * v
     for name, v in ks(Lr).items():
         out[name] += B * v
-    # keys are read once per launch: relinearization key + one Galois key per group
-    out["ks_inner_product"] += 2 * L * (L + 1) * n * W + len(STEPS_K) * 2 * Lr * (Lr + 1) * n * W
+    # keys are read once per launch: relinearization key + one Galois key per group; the
+    # inner product reads their data-modulus columns, the special transform the last one
+    out["ks_inner_product"] += 2 * L * L * n * W + len(STEPS_K) * 2 * Lr * Lr * n * W
+    out["ks_special_intt"] += 2 * L * n * W + len(STEPS_K) * 2 * Lr * n * W
     return out
 
 
