@@ -131,10 +131,12 @@ struct ModUpOp {
     const uint64_t *chain;    // device copy of chain values (for the reduce test)
     int L, K, ckks, logn;
     // Up to 15 digits are summed unreduced by the 128-bit inner products: below 4q (a
-    // 61-bit q), below 16 q (q < 2^60, deferred reductions) or below 38 q (q < 2^58, no
-    // subtraction at all): 15 products below 4 q * q < 2^124, 16 q * q < 2^124 or
-    // 38 q * q < 2^121.3 each stay below 2^128. More digits are reduced to [0, q) at the
-    // store (the transform then stays below 16 q).
+    // 61-bit q), below 16 q (q < 2^60, deferred reductions), or, for q < 2^58 in the
+    // one-CTA transform (no subtraction at all), below 2^61 + 28 q < 2^63.1: the digit
+    // then enters unreduced (below q_j < 2^61) and the transform's 14 stages add at most
+    // 2q each. 15 products below 4 q * q < 2^124, 16 q * q < 2^124 or 2^63.1 * 2^58 stay
+    // below 2^128. More digits are reduced to [0, q) at the store (the transform then
+    // stays below 16 q).
     static constexpr int LAZY_MAX_L = 15;
     static constexpr bool wide_slack = true;
     struct Ctx {
@@ -162,8 +164,11 @@ struct ModUpOp {
         Ctx c;
         c.lm = make_limb(m, 0);
         c.ratio_hi = m.ratio_hi;
-        c.reduce = mods[j].value > m.value;
-        c.slack = (L <= LAZY_MAX_L && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        // the transform's input: any digit word in the no-subtraction form, below 4q in
+        // the others (a Barrett remainder in [0, 2q) when q_j is larger)
+        const bool wide = L <= LAZY_MAX_L && logn <= MAX_LOGB && m.value < (1ull << 58);
+        c.slack = wide ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.reduce = !wide && mods[j].value > 4 * m.value;
         c.in = src + (size_t)cb * sstride + ((size_t)j << logn);
         c.out = digits + ((((size_t)cb * L + j) * (L + 1) + i) << logn);
         return c;
@@ -361,7 +366,8 @@ struct ModDownBase {
         uint64_t ratio_hi;
         DropC d;
         int reduce;
-        int slack;   // forward transform (CKKS) with deferred reductions: outputs below 16 q or 38 q
+        int slack;   // forward transform (CKKS) with deferred reductions
+        uint64_t wide_off;   // (floor(2^64 / q_j) - 1) q_j: the epilogue's offset after the wide form
     };
     static constexpr bool wide_slack = true;
     __device__ Ctx make(int b) const {
@@ -373,7 +379,8 @@ struct ModDownBase {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)K * K + j];
         c.reduce = mods[K - 1].value > m.value;
-        c.slack = m.value < (1ull << 58) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.wide_off = (m.ratio_hi - 1) * m.value;
         c.acc = acc + (((size_t)bc * (L + 1) + j) << logn);
         c.last = last + ((size_t)bc << logn);
         c.ct = ct + (size_t)cb * cstride + (((size_t)cc * L + j) << logn);
@@ -392,14 +399,18 @@ struct ModDownBase {
 };
 
 // Step 5, CKKS: NTT of (r mod q_j) + fix, epilogue ct += (acc + 4 q_j - ntt) * q_k^-1.
-// After a transform with deferred reductions (ntt below 16 q_j, or 38 q_j for q_j <
-// 2^58) one subtraction of 8 q_j (32 q_j) brings ntt below 8 q_j (32 q_j) and the
-// epilogue takes acc + 8 q_j - ntt (acc + 32 q_j - ntt): below 9 q_j (33 q_j) < 2^64,
-// where acc + 16 q_j - ntt would pass 2^64 for a 60-bit q_j. The same residue each way.
-// The transform's input only has to stay below 4 q_j: a lazy residue (< 2 q_j) plus fix.
+// The transform's input only has to stay below 4 q_j: a lazy residue (< 2 q_j) plus fix
+// (at most q_j). After the deferred-reduction form (ntt below 16 q_j) one subtraction of
+// 8 q_j brings ntt below 8 q_j and the epilogue takes acc + 8 q_j - ntt: below 9 q_j <
+// 2^64, where acc + 16 q_j - ntt would pass 2^64 for a 60-bit q_j. The no-subtraction
+// form (q_j < 2^58, one CTA per limb) takes r itself (below 2^61) plus fix: ntt stays
+// below 2^61 + 29 q_j < 2^63.3 < 2^64 - 2 q_j <= wide_off, and the epilogue takes
+// acc + wide_off - ntt, below 2^64. The same residue each way.
 struct ModDownCkksOp : ModDownBase {
     __device__ Ctx ctx(int b) const { return make(b); }
-    __device__ uint64_t load(const Ctx &c, int e) const { return last_mod_lazy(c, e) + c.d.fix; }
+    __device__ uint64_t load(const Ctx &c, int e) const {
+        return (c.slack == SLACK_WIDE ? c.last[e] : last_mod_lazy(c, e)) + c.d.fix;
+    }
     // epilogue reads of a coefficient pair: the accumulator and the ciphertext limb
     struct Epi {
         ulonglong2 acc, ct;
@@ -409,8 +420,8 @@ struct ModDownCkksOp : ModDownBase {
     }
     __device__ uint64_t fin(const Ctx &c, uint64_t acc, uint64_t ct, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        const int sh = c.slack == SLACK_WIDE ? 5 : c.slack ? 3 : 2;
-        const uint64_t x = acc + (q << sh) - (c.slack ? csub(v, q << sh) : v);
+        const uint64_t x = c.slack == SLACK_WIDE ? acc + c.wide_off - v
+                           : c.slack ? acc + (q << 3) - csub(v, q << 3) : acc + (q << 2) - v;
         return add_mod(mul_shoup(x, c.d.inv, c.d.inv_quo, q), ct, q);
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {

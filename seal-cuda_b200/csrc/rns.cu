@@ -106,7 +106,8 @@ struct RescaleNttOp {
         uint64_t ratio_hi;
         DropC d;
         int reduce;
-        int slack;   // forward transform with deferred reductions: outputs below 16 q or 38 q
+        int slack;   // forward transform with deferred reductions
+        uint64_t wide_off;   // (floor(2^64 / q_j) - 1) q_j: the epilogue's offset after the wide form
     };
     static constexpr bool wide_slack = true;
     __device__ Ctx ctx(int b) const {
@@ -117,7 +118,8 @@ struct RescaleNttOp {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)L * K + j];
         c.reduce = mods[L - 1].value > m.value;
-        c.slack = m.value < (1ull << 58) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.wide_off = (m.ratio_hi - 1) * m.value;
         const size_t cb = p / size, k = p % size;
         c.in = in + cb * istride + ((k * L + j) << logn);
         c.out = out + cb * ostride + ((k * (L - 1) + j) << logn);
@@ -125,9 +127,11 @@ struct RescaleNttOp {
         return c;
     }
     // the transform takes any input below 4 q_j: the Barrett remainder (< 2 q_j) plus fix
+    // (at most q_j); the no-subtraction form (q_j < 2^58, one CTA per limb) takes r itself
+    // (below 2^61) plus fix
     __device__ uint64_t load(const Ctx &c, int e) const {
         uint64_t x = c.r[e];
-        if (c.reduce) x = x - mulhi(x, c.ratio_hi) * c.lm.q;
+        if (c.reduce && c.slack != SLACK_WIDE) x = x - mulhi(x, c.ratio_hi) * c.lm.q;
         return x + c.d.fix;
     }
     // epilogue reads of a coefficient pair: the limb being rescaled
@@ -137,11 +141,12 @@ struct RescaleNttOp {
     __device__ Epi epi2(const Ctx &c, int e) const { return {*reinterpret_cast<const ulonglong2 *>(c.in + e)}; }
     __device__ uint64_t fin(const Ctx &c, uint64_t in, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        // after deferred reductions v is below 16 q (38 q for q < 2^58): one subtraction
-        // of 8 q (32 q) keeps in + 8 q - v (in + 32 q - v) below 9 q (33 q) < 2^64
-        // (in + 16 q - v would pass 2^64 for a 60-bit q)
-        const int sh = c.slack == SLACK_WIDE ? 5 : c.slack ? 3 : 2;
-        const uint64_t x = in + (q << sh) - (c.slack ? csub(v, q << sh) : v);
+        // after deferred reductions v is below 16 q: one subtraction of 8 q keeps
+        // in + 8 q - v below 9 q < 2^64 (in + 16 q - v would pass 2^64 for a 60-bit q);
+        // after the no-subtraction form v is below 2^61 + 29 q < 2^63.3 < wide_off, and
+        // in + wide_off - v stays below 2^64
+        const uint64_t x = c.slack == SLACK_WIDE ? in + c.wide_off - v
+                           : c.slack ? in + (q << 3) - csub(v, q << 3) : in + (q << 2) - v;
         return mul_shoup(x, c.d.inv, c.d.inv_quo, q);
     }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b, const Epi &p) const {

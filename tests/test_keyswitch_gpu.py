@@ -263,3 +263,39 @@ def test_keyswitch_slack_bounds(orc, scheme):
         ctx("keyswitch", L, _dev(target), 0, dct, 0, dkey, 1, None)
         exp = orc.keyswitch(scheme, logn, data + [moduli[-1]], t, target[0], ct[0], _key_sub(key, L))
         assert np.array_equal(_host(dct)[0], exp), L
+
+
+def test_wide_form_takes_unreduced_inputs(orc):
+    """Limbs of moduli below 2^58 run the one-CTA forward transforms with no subtraction
+    and take their inputs unreduced: the mod-up the digit of a larger modulus, the CKKS
+    mod-down and rescale the 60-bit residue being dropped. Chain {57, 57, 60} + a 60-bit
+    special prime at N = 16384: key switching (60-bit digit into 57-bit moduli, special
+    residue into 57-bit limbs) and rescaling (the 60-bit last limb into 57-bit limbs),
+    with residues near q, bit-exact against the oracle."""
+    n = 16384
+    logn = n.bit_length() - 1
+    moduli = orc.coeff_modulus_create(n, [57, 57, 60, 60])
+    assert moduli[0] < (1 << 58) and moduli[2] >= (1 << 59)
+    ctx = tb_capi.Context(CKKS, n, moduli, 0)
+    K, L = len(moduli), len(moduli) - 1
+    rng = np.random.default_rng(57)
+
+    def near_q(mods, lead):
+        return np.stack([rng.integers(q - (q >> 6), q, tuple(lead) + (n,), dtype=np.uint64) for q in mods], axis=-2)
+
+    key = near_q(moduli, (K - 1, 2))
+    data = moduli[:L]
+    target = near_q(data, (2,))
+    ct = near_q(data, (2, 2))
+    dct = _dev(ct)
+    ctx("keyswitch", L, _dev(target), 0, dct, 0, _dev(key), 2, None)
+    got = _host(dct)
+    for b in range(2):
+        exp = orc.keyswitch(CKKS, logn, data + [moduli[-1]], 0, target[b], ct[b], _key_sub(key, L))
+        assert np.array_equal(got[b], exp), b
+    x = near_q(data, (3,))
+    out = torch.empty((3, L - 1, n), dtype=torch.int64, device="cuda")
+    ctx("rescale_to_next", L, _dev(x), 0, out, 0, 1, 3, None)
+    got = _host(out)
+    for p in range(3):
+        assert np.array_equal(got[p], orc.rns_op("div_round_last_ntt", n, data, 0, x[p], L)[: L - 1]), p
