@@ -75,6 +75,27 @@ __device__ __forceinline__ uint64_t mul_mod(uint64_t a, uint64_t b, const Mod &m
     return reduce128(mulhi(a, b), a * b, m);
 }
 
+// (hi:lo) mod q for a value below 2^(2n+1), n the bit length of q (n <= 61): a product
+// of two residues below q, or the sum of two such products. Barrett with one 64-bit
+// quotient product instead of reduce128's three 128-bit ones: with s = n - 2,
+// t = (hi:lo) >> s < 2^(n+3) <= 2^64 and mu = floor(2^(64+s) / q) = floor(2^128 / q) >>
+// (64 - s) < 2^63, the estimate floor(t mu / 2^64) is never above floor(x / q) and at
+// most 2 below it (it misses x / 2^(s+64) < 2^(n-61) <= 1, 2^s / q < 1/2 and the
+// floors), so x - estimate * q lies in [0, 3q) and two conditional subtractions finish.
+__device__ __forceinline__ uint64_t reduce_prod(uint64_t hi, uint64_t lo, const Mod &m) {
+    const uint64_t q = m.value;
+    const int s = 62 - __clzll((long long)q);
+    const uint64_t t = s ? (lo >> s) | (hi << (64 - s)) : lo;
+    const uint64_t mu = s ? (m.ratio_hi << s) | (m.ratio_lo >> (64 - s)) : m.ratio_hi;
+    const uint64_t r = lo - mulhi(t, mu) * q;
+    return csub(csub(r, 2 * q), q);
+}
+
+// a * b mod q for residues a, b < q.
+__device__ __forceinline__ uint64_t mul_mod_canon(uint64_t a, uint64_t b, const Mod &m) {
+    return reduce_prod(mulhi(a, b), a * b, m);
+}
+
 // 128-bit accumulator helpers for lazy inner products.
 struct U128 {
     uint64_t lo, hi;

@@ -19,7 +19,7 @@ unsigned grid_for(uint64_t work, int threads);
 void ensure_pool_retains(int device);
 int tensor_product_mods(const Context &c, const Mod *mods, int L, const uint64_t *a, uint64_t astride,
                         const uint64_t *b, uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B,
-                        cudaStream_t s);
+                        cudaStream_t s, bool canon = false);
 
 // ---------------------------------------------------------- level constants
 
@@ -455,7 +455,9 @@ int multiply(const Context &c, int L, const uint64_t *a, uint64_t astride, const
     if (!astride) astride = 2ull * L * n;
     if (!bstride) bstride = 2ull * L * n;
     if (!ostride) ostride = 3ull * L * n;
-    if (c.scheme == SCHEME_CKKS) return tensor_product_mods(c, c.d_mods, L, a, astride, b, bstride, out, ostride, B, s);
+    // CKKS: the NTT-domain tensor of two ciphertexts, whose words are residues below q
+    if (c.scheme == SCHEME_CKKS)
+        return tensor_product_mods(c, c.d_mods, L, a, astride, b, bstride, out, ostride, B, s, true);
     if (c.scheme != SCHEME_BFV && c.scheme != SCHEME_BGV) return set_error(TB_ERR_UNSUPPORTED, "scheme has no multiply");
     if (c.logn > MAX_FUSED_LOGN) return set_error(TB_ERR_UNSUPPORTED, "multiply supports N <= 131072");
     ensure_pool_retains(c.device);

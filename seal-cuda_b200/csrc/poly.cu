@@ -56,7 +56,11 @@ void ensure_pool_retains(int device) {
 
 // Ciphertext tensor product of two size-2 ciphertexts in the NTT domain
 // (Evaluator::ckksMultiply, src/evaluator.cpp:626-702):
-// d0 = a0 b0, d1 = a0 b1 + a1 b0, d2 = a1 b1 per limb.
+// d0 = a0 b0, d1 = a0 b1 + a1 b0, d2 = a1 b1 per limb. CANON: the words are residues
+// below q (a valid ciphertext's), so every product is below q^2 and d1's sum below
+// 2 q^2, reduce_prod's range; otherwise (lazy transform outputs of the BFV and BGV
+// multiplies, any words of tb_tensor_product) the general 128-bit reduction.
+template <bool CANON>
 __global__ void tensor_kernel(const uint64_t *__restrict__ a, uint64_t astride, const uint64_t *__restrict__ b,
                               uint64_t bstride, uint64_t *__restrict__ out, uint64_t ostride,
                               const Mod *__restrict__ mods, int first, int L, int logn, uint64_t B) {
@@ -89,19 +93,33 @@ __global__ void tensor_kernel(const uint64_t *__restrict__ a, uint64_t astride, 
         mac128(s0, a1.x, b0.x);
         mac128(s1, a0.y, b1.y);
         mac128(s1, a1.y, b0.y);
-        *reinterpret_cast<ulonglong2 *>(po) = make_ulonglong2(mul_mod(a0.x, b0.x, m), mul_mod(a0.y, b0.y, m));
-        *reinterpret_cast<ulonglong2 *>(po + pl) = make_ulonglong2(reduce128(s0.hi, s0.lo, m), reduce128(s1.hi, s1.lo, m));
-        *reinterpret_cast<ulonglong2 *>(po + 2 * pl) = make_ulonglong2(mul_mod(a1.x, b1.x, m), mul_mod(a1.y, b1.y, m));
+        if constexpr (CANON) {
+            *reinterpret_cast<ulonglong2 *>(po) =
+                make_ulonglong2(mul_mod_canon(a0.x, b0.x, m), mul_mod_canon(a0.y, b0.y, m));
+            *reinterpret_cast<ulonglong2 *>(po + pl) =
+                make_ulonglong2(reduce_prod(s0.hi, s0.lo, m), reduce_prod(s1.hi, s1.lo, m));
+            *reinterpret_cast<ulonglong2 *>(po + 2 * pl) =
+                make_ulonglong2(mul_mod_canon(a1.x, b1.x, m), mul_mod_canon(a1.y, b1.y, m));
+        } else {
+            *reinterpret_cast<ulonglong2 *>(po) = make_ulonglong2(mul_mod(a0.x, b0.x, m), mul_mod(a0.y, b0.y, m));
+            *reinterpret_cast<ulonglong2 *>(po + pl) =
+                make_ulonglong2(reduce128(s0.hi, s0.lo, m), reduce128(s1.hi, s1.lo, m));
+            *reinterpret_cast<ulonglong2 *>(po + 2 * pl) = make_ulonglong2(mul_mod(a1.x, b1.x, m), mul_mod(a1.y, b1.y, m));
+        }
     }
 }
 
-// Tensor product with limb l reduced by mods[l] (chain prefix or a Bsk array).
+// Tensor product with limb l reduced by mods[l] (chain prefix or a Bsk array); canon:
+// every input word is a residue below its modulus.
 int tensor_product_mods(const Context &c, const Mod *mods, int L, const uint64_t *a, uint64_t astride,
                         const uint64_t *b, uint64_t bstride, uint64_t *out, uint64_t ostride, uint64_t B,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool canon) {
     TraceScope ts("tensor", s);
-    tensor_kernel<<<grid_for(B * L * c.n / 2, 256), 256, 0, s>>>(a, astride, b, bstride, out, ostride, mods, 0, L,
-                                                                 c.logn, B);
+    const unsigned grid = grid_for(B * L * c.n / 2, 256);
+    if (canon)
+        tensor_kernel<true><<<grid, 256, 0, s>>>(a, astride, b, bstride, out, ostride, mods, 0, L, c.logn, B);
+    else
+        tensor_kernel<false><<<grid, 256, 0, s>>>(a, astride, b, bstride, out, ostride, mods, 0, L, c.logn, B);
     return status_from(cudaGetLastError());
 }
 
@@ -115,7 +133,7 @@ int tensor_product(const Context &c, int first, int L, const uint64_t *a, uint64
     if (!astride) astride = 2ull * L * n;
     if (!bstride) bstride = 2ull * L * n;
     if (!ostride) ostride = 3ull * L * n;
-    return tensor_product_mods(c, c.d_mods + first, L, a, astride, b, bstride, out, ostride, B, s);
+    return tensor_product_mods(c, c.d_mods + first, L, a, astride, b, bstride, out, ostride, B, s, false);
 }
 
 }  // namespace tb

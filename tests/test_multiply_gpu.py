@@ -82,3 +82,33 @@ def test_bgv_and_ckks_multiply(orc):
             if scheme == BGV:
                 exp = orc.ntt_inverse_rns(logn, data, exp)
             assert np.array_equal(got[i], exp), (scheme, i)
+
+
+@pytest.mark.parametrize("bits", [[60, 60, 60, 60], [20, 30, 50, 60], [30, 41, 40, 60]])
+def test_ckks_multiply_extreme_words(orc, bits):
+    """The CKKS tensor reduces its products with the one-product Barrett reduction (valid
+    below 2^(2n+1)); its extremes: every word q - 1 (products (q - 1)^2, sums 2 (q - 1)^2),
+    zeros, and words near q, for moduli of 20 .. 60 bits. Checked against the oracle's
+    dyadic products."""
+    n = 4096
+    moduli = orc.coeff_modulus_create(n, bits)
+    L, B = len(moduli) - 1, 3
+    data = moduli[:L]
+    qs = np.asarray(data, np.uint64)[None, None, :, None]
+    rng = np.random.default_rng(61)
+    a = np.broadcast_to(qs - 1, (B, 2, L, n)).copy()
+    b = a.copy()
+    a[1] = 0
+    a[2] = (qs - 1 - (rng.integers(0, 1 << 16, (2, L, n), dtype=np.uint64) % qs))[0]
+    b[2] = (qs - 1 - (rng.integers(0, 1 << 16, (2, L, n), dtype=np.uint64) % qs))[0]
+    ctx = tb_capi.Context(CKKS, n, moduli, 0)
+    out = torch.empty((B, 3, L, n), dtype=torch.int64, device="cuda")
+    ctx("multiply", L, _dev(a), 0, _dev(b), 0, out, 0, B, None)
+    got = _host(out)
+    for i in range(B):
+        x, y = a[i], b[i]
+        d0 = orc.dyadic_rns(data, x[0], y[0])
+        d2 = orc.dyadic_rns(data, x[1], y[1])
+        s1 = orc.dyadic_rns(data, x[0], y[1]).astype(object) + orc.dyadic_rns(data, x[1], y[0]).astype(object)
+        d1 = np.stack([(s1[l] % data[l]).astype(np.uint64) for l in range(L)])
+        assert np.array_equal(got[i], np.stack([d0, d1, d2])), i
