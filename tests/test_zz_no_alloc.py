@@ -69,3 +69,59 @@ def test_noalloc_rejects_levels_beyond_its_scratch():
     with pytest.raises(tb_capi.TroyError) as e:
         ctx("relinearize_noalloc", K - 1, ct, 0, key, 1, None)
     assert e.value.status == 1 and "static scratch" in str(e.value)
+
+
+_CHILD = r"""
+import sys
+import numpy as np
+import torch
+import tb_capi
+from oracle import Oracle
+orc = Oracle("orc")
+n, batch = 4096, 3
+moduli = orc.coeff_modulus_create(n, [60, 40, 40, 60])
+ctx = tb_capi.Context(tb_capi.SCHEME_CKKS, n, moduli)
+K = len(moduli)
+L = K - 1
+rng = np.random.default_rng(4096)
+def rand(mods, lead):
+    out = np.empty(tuple(lead) + (len(mods), n), np.uint64)
+    for i, q in enumerate(mods):
+        out[..., i, :] = rng.integers(0, q, tuple(lead) + (n,), dtype=np.uint64)
+    return torch.from_numpy(out.view(np.int64)).cuda()
+key = rand(moduli, (K - 1, 2))
+src = rand(moduli[:L], (batch, 3))
+got = torch.empty_like(src)
+graph = torch.cuda.CUDAGraph()
+side = torch.cuda.Stream()
+side.wait_stream(torch.cuda.current_stream())
+torch.cuda.synchronize()
+with torch.cuda.graph(graph, stream=side):   # the process's first library call
+    got.copy_(src)
+    ctx("relinearize_noalloc", L, got, 0, key, batch, side)
+graph.replay()
+ref = src.clone()
+ctx("relinearize", L, ref, 0, key, batch, None)
+torch.cuda.synchronize()
+assert torch.equal(got[:, :2], ref[:, :2])
+print("CAPTURED-OK")
+"""
+
+
+def test_noalloc_first_call_inside_a_graph_capture():
+    """The static scratch's device address is taken when the context is created, so in a
+    fresh process the first relinearize_noalloc call loads and allocates nothing: it can
+    be the process's first library call, inside a CUDA graph capture (a call that loaded
+    the module or allocated would break the capture). The replayed graph gives the words
+    of tb_relinearize. Runs in a child process so that no earlier test has loaded the
+    module."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.pathsep.join([os.path.join(root, "seal-cuda_b200", "python"), os.path.join(root, "oracle"),
+                                         os.path.join(root, "seal-cuda_b200", "lib"), env.get("PYTHONPATH", "")])
+    r = subprocess.run([sys.executable, "-c", _CHILD], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "CAPTURED-OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
