@@ -504,7 +504,8 @@ def run_uneven(total=512, reps=5):
     {4096, 8192, 16384} (3 / 5 / 9 primes; BFV, BGV, BFV), multiply -> relinearize ->
     rotate_rows(1), seeded uniform residues as ciphertexts and keys. Reports ops/s of
     the captured CUDA graph (one launch per batch), of the stream-overlapped calls and
-    of the one-ciphertext-per-call path (each the best of three timings)."""
+    of the one-ciphertext-per-call path (each the best of three timings), and of the
+    reference's own CUDA path one pair per call at the same shapes and counts."""
     import numpy as np
     import torch
     import tb_capi
@@ -515,7 +516,7 @@ def run_uneven(total=512, reps=5):
     gen = torch.Generator(device="cuda")
     gen.manual_seed(99)
     lib = tb_capi.lib()
-    groups = []
+    groups, shapes = [], []
     for gi, (scheme, n, bits) in enumerate(UNEVEN_SHAPES):
         arr = (ctypes.c_int * len(bits))(*bits)
         mods = (ctypes.c_uint64 * len(bits))()
@@ -525,6 +526,7 @@ def run_uneven(total=512, reps=5):
         tb_capi.check(lib.tb_plain_modulus_batching(ctypes.c_uint64(16384), 20, ctypes.byref(tmod)))
         ctx = tb_capi.Context(scheme, n, moduli, tmod.value)
         K, L, cnt = len(moduli), len(moduli) - 1, int((draws == gi).sum())
+        shapes.append((scheme, n, moduli, tmod.value, cnt))
         e = ctypes.c_uint32()
         ctx("galois_elt_from_step", 1, ctypes.byref(e))
         groups.append(ShapeGroup(ctx, L, _rand_residues(torch, (cnt, 2, L, n), moduli[:L], gen),
@@ -562,14 +564,58 @@ def run_uneven(total=512, reps=5):
     shaped.capture()
     ms_shapes_graph = timed(shaped.replay, reps)
     best = min(ms_graph, ms_shapes_graph)
-    return {"workload": "uneven_bfv_bgv_n4096_8192_16384_mul_relin_rotate", "ciphertexts": total,
-            "groups": {f"N={g.ctx.n},L={g.L}": g.count for g in groups},
-            "graph_ops_per_s": round(total / (ms_graph * 1e-3), 1),
-            "streams_ops_per_s": round(total / (ms_streams * 1e-3), 1),
-            "shapes_ops_per_s": round(total / (ms_shapes * 1e-3), 1),
-            "shapes_graph_ops_per_s": round(total / (ms_shapes_graph * 1e-3), 1),
-            "per_op_ops_per_s": round(total / (ms_per_op * 1e-3), 1),
-            "graph_over_per_op": round(ms_per_op / best, 2)}
+    out = {"workload": "uneven_bfv_bgv_n4096_8192_16384_mul_relin_rotate", "ciphertexts": total,
+           "groups": {f"N={g.ctx.n},L={g.L}": g.count for g in groups},
+           "graph_ops_per_s": round(total / (ms_graph * 1e-3), 1),
+           "streams_ops_per_s": round(total / (ms_streams * 1e-3), 1),
+           "shapes_ops_per_s": round(total / (ms_shapes * 1e-3), 1),
+           "shapes_graph_ops_per_s": round(total / (ms_shapes_graph * 1e-3), 1),
+           "per_op_ops_per_s": round(total / (ms_per_op * 1e-3), 1),
+           "graph_over_per_op": round(ms_per_op / best, 2)}
+    ref = reference_gpu_uneven(shapes)
+    if ref is not None:
+        out["reference_gpu_per_op"] = ref
+        if "ms_per_batch" in ref:
+            out["graph_over_reference_gpu_per_op"] = round(ref["ms_per_batch"] / best, 2)
+    return out
+
+
+def _ref_gpu_uneven_worker(args):
+    """Child process: the reference's CUDA evaluator one ciphertext pair per call at each
+    shape of the uneven batch (ms per op, decrypted result checked)."""
+    shapes, ops = args
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libtroyref_gpu.so"))
+    lib.ref_gpu_batch_chain.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int,
+                                        ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int)]
+    res = []
+    for scheme, n, moduli, t, _ in shapes:
+        arr = (ctypes.c_uint64 * len(moduli))(*moduli)
+        ms, ok = ctypes.c_double(), ctypes.c_int()
+        rc = lib.ref_gpu_batch_chain(scheme, n, arr, len(moduli), t, ops, ctypes.byref(ms), ctypes.byref(ok))
+        res.append((rc, ms.value, ok.value))
+    return res
+
+
+def reference_gpu_uneven(shapes, ops=8):
+    """The reference's own CUDA path on the uneven batch's chain (multiply, relinearize,
+    rotate rows), one ciphertext pair per call, at each shape: the batch's time is each
+    group's count times that shape's time per op. None when that library is not built."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libtroyref_gpu.so")):
+        return None
+    with mp.get_context("spawn").Pool(1) as pool:
+        res = pool.apply(_ref_gpu_uneven_worker, ((shapes, ops),))
+    if any(rc == 1 or ms <= 0 for rc, ms, _ in res):
+        return {"unavailable": "reference CUDA path raised an exception"}
+    ms_batch = sum(cnt * ms for (_, _, _, _, cnt), (_, ms, _) in zip(shapes, res))
+    total = sum(cnt for *_, cnt in shapes)
+    return {"ops_per_s": round(total / (ms_batch * 1e-3), 1), "ms_per_batch": round(ms_batch, 3),
+            "ms_per_op": {f"N={n}": round(ms, 3) for (_, n, *_), (_, ms, _) in zip(shapes, res)},
+            "decrypts_correctly": all(ok == 1 for *_, ok in res),
+            "form": "reference EvaluatorCuda compiled for sm_100a, one pair per call, "
+                    f"{ops} ops per shape after 2 warm-up ops, in a child process"}
 
 
 def _pinned(a):

@@ -4,6 +4,7 @@
 // pair per call — multiply, relinearizeInplace, rescaleToNextInplace,
 // rotateVectorInplace — the "plain per-op GPU path" the batched library is compared
 // with. The decrypted result of the last op is checked against the FP64 product.
+// ref_gpu_batch_chain does the same for BFV / BGV (multiply, relinearize, rotate rows).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -86,6 +87,79 @@ extern "C" int ref_gpu_ckks_chain(size_t n, const uint64_t *moduli, int count, i
             err = std::max(err, std::abs(got[i] - v[j] * w[j]));
         }
         *max_err = err;
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    } catch (...) {
+        return 1;
+    }
+}
+
+// The same for BFV / BGV (scheme 1 / 3) with plain modulus t: multiply,
+// relinearizeInplace, rotateRowsInplace(1) one ciphertext pair per call (the uneven
+// batch's chain at one of its shapes). *ok = 1 when the last op decrypts to the slot
+// products rotated by one inside each row.
+extern "C" int ref_gpu_batch_chain(int scheme, size_t n, const uint64_t *moduli, int count, uint64_t t, int ops,
+                                   double *ms_per_op, int *ok) {
+    try {
+        KernelProvider::initialize();
+        EncryptionParameters parms((SchemeType)scheme);
+        parms.setPolyModulusDegree(n);
+        std::vector<Modulus> q;
+        for (int i = 0; i < count; i++) q.emplace_back(moduli[i]);
+        parms.setCoeffModulus(q);
+        parms.setPlainModulus(t);
+        SEALContext context(parms, true, SecurityLevel::none);
+        BatchEncoder encoder(context);
+        KeyGenerator keygen(context);
+        PublicKey pk;
+        keygen.createPublicKey(pk);
+        RelinKeys rlk = keygen.createRelinKeys();
+        GaloisKeys gk = keygen.createGaloisKeys(std::vector<int>{1});
+        Encryptor encryptor(context, pk);
+        Decryptor decryptor(context, keygen.secretKey());
+        Evaluator ev(context);
+        std::mt19937_64 gen(11);
+        std::vector<uint64_t> v(n), w(n);
+        for (size_t i = 0; i < n; i++) {
+            v[i] = gen() % t;
+            w[i] = gen() % t;
+        }
+        Plaintext pv, pw;
+        encoder.encode(v, pv);
+        encoder.encode(w, pw);
+        Ciphertext a, b;
+        encryptor.encrypt(pv, a);
+        encryptor.encrypt(pw, b);
+        auto chain = [&](Ciphertext &m) {
+            ev.multiply(a, b, m);
+            ev.relinearizeInplace(m, rlk);
+            ev.rotateRowsInplace(m, 1, gk);
+        };
+        Ciphertext m;
+        for (int i = 0; i < 2; i++) chain(m);  // warm-up
+        cudaDeviceSynchronize();
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, 0);
+        for (int i = 0; i < ops; i++) chain(m);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms_per_op = ms / ops;
+        Plaintext p;
+        decryptor.decrypt(m, p);
+        std::vector<uint64_t> got;
+        encoder.decode(p, got);
+        const size_t half = n / 2;
+        int good = got.size() == n;
+        for (size_t i = 0; good && i < n; i++) {
+            const size_t row = i / half, j = row * half + (i % half + 1) % half;
+            good = got[i] == (uint64_t)((unsigned __int128)v[j] * w[j] % t);
+        }
+        *ok = good;
         return cudaGetLastError() == cudaSuccess ? 0 : 2;
     } catch (...) {
         return 1;
