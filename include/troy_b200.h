@@ -137,6 +137,9 @@ int tb_multiply_sizes(tb_context *ctx, int L, const uint64_t *a, int a_size, con
  * adds switch(target) into the ciphertext's first two polynomials. target[b] has L
  * limbs at target + b*target_stride (NTT form for CKKS, coefficient form for
  * BFV/BGV); ciphertext b at ct + b*ct_stride. Strides in words, 0 = packed.
+ * Every target and ciphertext word is a residue below its limb's modulus (as in any
+ * valid ciphertext; the transforms take the target words unreduced). The same holds
+ * for the ciphertexts of tb_relinearize, tb_apply_galois and tb_multiply.
  * Replaces EvaluatorCuda::switchKeyInplace (src/evaluator_cuda.cu:1164-1363).
  */
 int tb_keyswitch(tb_context *ctx, int L, const uint64_t *target, uint64_t target_stride, uint64_t *ct,
