@@ -319,8 +319,9 @@ def run_b200(args, rank, world):
     PC = PAIRS // CH
     chunk_runs = [stepper.runs(c * PC, PC) for c in range(CH)]
 
-    def chunk_step(c, a, b, out, st=stream):
-        stepper.chain(chunk_runs[c], PC, slice(0, PC), a, b, out, st)
+    def chunk_step(c, j, a, b, out, st):
+        # chunks on compute stream j use the step's scratch rows j*PC .. (j+1)*PC - 1
+        stepper.chain(chunk_runs[c], PC, slice(j * PC, (j + 1) * PC), a, b, out, st)
 
     hA = torch.empty(A.shape, dtype=torch.int64, pin_memory=True)
     hB = torch.empty(B.shape, dtype=torch.int64, pin_memory=True)
@@ -331,6 +332,9 @@ def run_b200(args, rank, world):
     dB = [torch.empty_like(B[:PC]) for _ in range(2)]
     dO = [torch.empty_like(O[:PC]) for _ in range(2)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    # two compute streams: unit u computes on s_comp[u % 2] with buffers [u % 2], so one
+    # chunk's short launches overlap the next chunk's, as the sub-batches of the step do
+    s_comp = [torch.cuda.Stream(), torch.cuda.Stream()]
     ev = lambda: torch.cuda.Event()
     pending = {}
 
@@ -362,14 +366,15 @@ def run_b200(args, rank, world):
                 dA[j].copy_(hA[rows], non_blocking=True)
                 dB[j].copy_(hB[rows], non_blocking=True)
             arrived.record(s_in)
-        stream.wait_event(arrived)
+        cs = s_comp[j]
+        cs.wait_event(arrived)
         if ("left", u - 2) in pending:
-            stream.wait_event(pending.pop(("left", u - 2)))          # dO[j] read out
+            cs.wait_event(pending.pop(("left", u - 2)))              # dO[j] read out
         if seeded["on"]:
-            ctx("expand_seeded_batch", L, dSA[j], PC, 0, dA[j][:, 1], 2 * L * N, stream)
-            ctx("expand_seeded_batch", L, dSB[j], PC, 0, dB[j][:, 1], 2 * L * N, stream)
-        chunk_step(c, dA[j], dB[j], dO[j])
-        computed.record(stream)
+            ctx("expand_seeded_batch", L, dSA[j], PC, 0, dA[j][:, 1], 2 * L * N, cs)
+            ctx("expand_seeded_batch", L, dSB[j], PC, 0, dB[j][:, 1], 2 * L * N, cs)
+        chunk_step(c, j, dA[j], dB[j], dO[j], cs)
+        computed.record(cs)
         with torch.cuda.stream(s_out):
             s_out.wait_event(computed)
             hO[k % 2][rows].copy_(dO[j], non_blocking=True)
@@ -379,9 +384,9 @@ def run_b200(args, rank, world):
 
     def e2e_run(first, count):
         start = ev()
-        start.record(stream)            # the copy streams begin after the timed start
-        s_in.wait_event(start)
-        s_out.wait_event(start)
+        start.record(stream)            # the copy and compute streams begin after the timed start
+        for st in (s_in, s_out, *s_comp):
+            st.wait_event(start)
         for k in range(first, first + count):
             for c in range(CH):
                 e2e_unit(k * CH + c, k, c)
@@ -396,6 +401,14 @@ def run_b200(args, rank, world):
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
+    # the host results of the last step equal the device-resident step's words (the
+    # chunks assign the rotation steps as the step's sub-batches do)
+    check = torch.empty_like(O)
+    step(A, B, check)
+    torch.cuda.synchronize()
+    if CH == SUB and not torch.equal(hO[(args.steps - 1) % 2], check.cpu()):
+        raise RuntimeError("end-to-end results differ from the device-resident step's")
+    del check
 
     # the same pipeline when the inputs arrive seed-compressed: half the input bytes
     seeded["on"] = True
