@@ -328,12 +328,14 @@ def run_b200(args, rank, world):
     hO = [torch.empty(O.shape, dtype=torch.int64, pin_memory=True) for _ in range(2)]
     hA.copy_(A)
     hB.copy_(B)
-    dA = [torch.empty_like(A[:PC]) for _ in range(2)]
-    dB = [torch.empty_like(B[:PC]) for _ in range(2)]
-    dO = [torch.empty_like(O[:PC]) for _ in range(2)]
+    NBUF = 3   # device buffer sets: a chunk's copy-in need not wait for the compute two chunks back
+    dA = [torch.empty_like(A[:PC]) for _ in range(NBUF)]
+    dB = [torch.empty_like(B[:PC]) for _ in range(NBUF)]
+    dO = [torch.empty_like(O[:PC]) for _ in range(NBUF)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    # two compute streams: unit u computes on s_comp[u % 2] with buffers [u % 2], so one
-    # chunk's short launches overlap the next chunk's, as the sub-batches of the step do
+    # two compute streams: unit u computes on s_comp[u % 2] (with the step's scratch rows
+    # of that stream), so one chunk's short launches overlap the next chunk's, as the
+    # sub-batches of the step do; its buffers are set u % NBUF
     s_comp = [torch.cuda.Stream(), torch.cuda.Stream()]
     ev = lambda: torch.cuda.Event()
     pending = {}
@@ -346,17 +348,17 @@ def run_b200(args, rank, world):
     hB0.copy_(B[:, 0])
     hSA = torch.arange(1, PAIRS + 1, dtype=torch.int64).mul_(7919).add_(1 << 40).pin_memory()
     hSB = torch.arange(1, PAIRS + 1, dtype=torch.int64).mul_(104729).add_(1 << 41).pin_memory()
-    dSA = [torch.empty((PC,), dtype=torch.int64, device="cuda") for _ in range(2)]
-    dSB = [torch.empty((PC,), dtype=torch.int64, device="cuda") for _ in range(2)]
+    dSA = [torch.empty((PC,), dtype=torch.int64, device="cuda") for _ in range(NBUF)]
+    dSB = [torch.empty((PC,), dtype=torch.int64, device="cuda") for _ in range(NBUF)]
     seeded = {"on": False}
 
     def e2e_unit(u, k, c):
-        j = u % 2
+        j, sc = u % NBUF, u % 2
         rows = slice(c * PC, (c + 1) * PC)
         arrived, computed, left = ev(), ev(), ev()
         with torch.cuda.stream(s_in):
-            if ("computed", u - 2) in pending:
-                s_in.wait_event(pending.pop(("computed", u - 2)))   # unit u-2 done reading dA[j], dB[j]
+            if ("computed", u - NBUF) in pending:
+                s_in.wait_event(pending.pop(("computed", u - NBUF)))  # unit u-NBUF done reading dA[j], dB[j]
             if seeded["on"]:
                 dA[j][:, 0].copy_(hA0[rows], non_blocking=True)
                 dB[j][:, 0].copy_(hB0[rows], non_blocking=True)
@@ -366,14 +368,14 @@ def run_b200(args, rank, world):
                 dA[j].copy_(hA[rows], non_blocking=True)
                 dB[j].copy_(hB[rows], non_blocking=True)
             arrived.record(s_in)
-        cs = s_comp[j]
+        cs = s_comp[sc]
         cs.wait_event(arrived)
-        if ("left", u - 2) in pending:
-            cs.wait_event(pending.pop(("left", u - 2)))              # dO[j] read out
+        if ("left", u - NBUF) in pending:
+            cs.wait_event(pending.pop(("left", u - NBUF)))           # dO[j] read out
         if seeded["on"]:
             ctx("expand_seeded_batch", L, dSA[j], PC, 0, dA[j][:, 1], 2 * L * N, cs)
             ctx("expand_seeded_batch", L, dSB[j], PC, 0, dB[j][:, 1], 2 * L * N, cs)
-        chunk_step(c, j, dA[j], dB[j], dO[j], cs)
+        chunk_step(c, sc, dA[j], dB[j], dO[j], cs)
         computed.record(cs)
         with torch.cuda.stream(s_out):
             s_out.wait_event(computed)
