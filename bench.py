@@ -429,6 +429,7 @@ def run_b200(args, rank, world):
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH,
             "int_ceiling": int_ceiling(lib, moduli[0]), "int_ceiling_slack": int_ceiling(lib, moduli[0], slack=True),
+            "mul64": mul64_rates(lib),
             "slack_share": slack_shares(moduli, L, N.bit_length() - 1), "sub": SUB}
 
 
@@ -840,6 +841,17 @@ def roofline(res, steps):
         out["int"] = {"achieved": round(rate / 1e9, 2), "peak": round(ceil / 1e9, 2), "unit": "Gbutterfly/s",
                       "frac": round(rate / ceil, 4), "butterflies_per_launch": round(bfly[name] * steps / launches),
                       "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
+        m = res.get("mul64")
+        if m:
+            # the machine bound: a butterfly's Shoup product is one high and two low 64-bit
+            # products; at the measured multiply throughputs no butterfly runs faster
+            bound = 1.0 / (1.0 / m["hi"] + 2.0 / m["lo"])
+            out["int"]["machine_bound"] = {
+                "mul_lo_per_s": round(m["lo"] / 1e9, 1), "mul_hi_per_s": round(m["hi"] / 1e9, 1), "unit": "G/s",
+                "butterflies_per_s": round(bound / 1e9, 2), "frac": round(rate / bound, 4),
+                "ceiling_frac": round(ceil / bound, 4),
+                "source": "tb_measure_mul64_rate: mul.lo.u64 / mul.hi.u64 in independent chains; "
+                          "bound = 1 / (1/hi + 2/lo) butterflies per second"}
         if name in res.get("slack_share", {}) and res.get("int_ceiling_slack"):
             out["int"]["peak_source"] = (
                 "measured here, operands in registers: tb_measure_butterfly_rate "
@@ -882,6 +894,20 @@ def fwd_subtracting_stages(logn, M=16):
         else:
             b, sub = M // 2 + 2, sub + 1
     return sub
+
+
+def mul64_rates(lib):
+    """The device's 64-bit multiply throughputs (tb_measure_mul64_rate): products per
+    second of mul.lo.u64 ("lo") and mul.hi.u64 ("hi")."""
+    fn = lib.tb_measure_mul64_rate
+    fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    out = {}
+    import tb_capi
+    for kind, key in ((0, "lo"), (1, "hi")):
+        r = ctypes.c_double(0)
+        tb_capi.check(fn(kind, None, ctypes.byref(r)))
+        out[key] = r.value
+    return out
 
 
 def slack_shares(moduli, L, logn):

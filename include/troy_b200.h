@@ -423,6 +423,13 @@ int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflie
    consumer, the 128-bit inner product, takes the unreduced outputs). No counterpart in
    the reference. */
 int tb_measure_slack_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
+/* The device's 64-bit integer multiply throughput in products per second: kind 0 the
+   low word (mul.lo.u64), kind 1 the high word (mul.hi.u64), each in long independent
+   chains at full occupancy. A Shoup product is one high and two low products, so
+   1 / (1 / hi + 2 / lo) bounds the butterflies per second of any transform built on it
+   (the bound the measured butterfly rates are set against). No counterpart in the
+   reference. */
+int tb_measure_mul64_rate(int kind, void *stream, double *products_per_second);
 /* Scratch budget of one key-switch launch sequence: a batch whose intermediates exceed
    it is processed in chunks (default 2 GiB, or the TB_KS_SCRATCH_BYTES environment
    value; 0 restores the default). */

@@ -198,9 +198,70 @@ int measure_butterfly_rate(uint64_t q, bool slack, cudaStream_t s, double *rate)
     return TB_OK;
 }
 
+// The machine's 64-bit integer multiply throughput, the arithmetic a butterfly is made
+// of (one high and two low 64 x 64-bit products per Shoup multiplication): 8 chains per
+// thread, every SM at full occupancy, of mul.lo.u64 (kind 0) or mul.hi.u64 (kind 1),
+// products per second. Each round multiplies every chain by its neighbour's previous
+// value, so no product can be folded into another (a chain x = x * b would be
+// reassociated by the compiler) and the 8 products of a round are independent.
+template <int KIND>
+__global__ void __launch_bounds__(256) mul64_rate_kernel(uint64_t *sink, uint64_t b, int rounds) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = b * (tid * 8u + (uint32_t)k + 1) | 1;
+    for (int r = 0; r < rounds; r++) {
+        uint64_t y[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) y[k] = x[k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if constexpr (KIND == 0) x[k] = y[k] * y[(k + 1) & 7];
+            else x[k] = __umul64hi(y[k], y[(k + 1) & 7]) ^ y[k];
+        }
+    }
+    uint64_t v = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) v ^= x[k];
+    sink[tid] = v;
+}
+
+int measure_mul64_rate(int kind, cudaStream_t s, double *rate) {
+    if (!rate || kind < 0 || kind > 1) return set_error(TB_ERR_INVALID_ARGUMENT, "kind is 0 (mul.lo.u64) or 1 (mul.hi.u64)");
+    const auto kernel = kind ? mul64_rate_kernel<1> : mul64_rate_kernel<0>;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    if (e != cudaSuccess) return status_from(e);
+    const unsigned blocks = (unsigned)(sms * std::max(per_sm, 1));
+    const int rounds = 4096;
+    uint64_t *sink = nullptr;
+    e = cudaMallocAsync(&sink, 8ull * blocks * 256, s);
+    if (e != cudaSuccess) return status_from(e);
+    int st = TB_OK;
+    const float ms = time_call(
+        [&] {
+            kernel<<<blocks, 256, 0, s>>>(sink, 0xd1b54a32d192ed03ull, rounds);
+            const cudaError_t le = cudaGetLastError();
+            return le == cudaSuccess ? TB_OK : status_from(le);
+        },
+        s, 3, st);
+    cudaFreeAsync(sink, s);
+    if (st != TB_OK) return st;
+    if (!(ms > 0)) return set_error(TB_ERR_CUDA, "no timing");
+    *rate = (double)blocks * 256.0 * rounds * 8.0 / (ms * 1e-3);
+    return TB_OK;
+}
+
 }  // namespace tb
 
 extern "C" {
+
+int tb_measure_mul64_rate(int kind, void *stream, double *products_per_second) {
+    return tb::measure_mul64_rate(kind, (cudaStream_t)stream, products_per_second);
+}
+
 
 int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second) {
     return tb::measure_butterfly_rate(modulus, false, (cudaStream_t)stream, butterflies_per_second);

@@ -47,3 +47,7 @@ def test_butterfly_rate_refuses_bad_moduli_on_the_host():
         for q in (0, 2, 1 << 40, (1 << 61) + 1):
             assert fn(q, None, ctypes.byref(r)) == 1
         assert b"2^61" in lib.tb_last_error()
+    lib.tb_measure_mul64_rate.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    r = ctypes.c_double(0)
+    for kind in (-1, 2):
+        assert lib.tb_measure_mul64_rate(kind, None, ctypes.byref(r)) == 1

@@ -240,3 +240,12 @@ def test_integer_ceiling_is_measured():
         assert 1e10 < r.value < 1e14
         rates.append(r.value)
     assert rates[1] > 0.95 * rates[0]
+    # the machine's 64-bit multiply throughputs bound both: a butterfly is one high and
+    # two low 64-bit products
+    mul = lib.tb_measure_mul64_rate
+    mul.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    lo, hi = ctypes.c_double(0), ctypes.c_double(0)
+    tb_capi.check(mul(0, None, ctypes.byref(lo)))
+    tb_capi.check(mul(1, None, ctypes.byref(hi)))
+    bound = 1.0 / (1.0 / hi.value + 2.0 / lo.value)
+    assert max(rates) <= 1.05 * bound, (rates, lo.value, hi.value)
