@@ -428,9 +428,9 @@ def run_b200(args, rank, world):
             "h2d_seeded": (hA0.numel() + hB0.numel() + hSA.numel() + hSB.numel()) * 8,
             "ms": ms, "e2e_ms": e2e_ms, "per_op_ms": per_op_ms, "per_op_pairs": per_op_pairs, "trace": trace, "launches": launches, "clocks": clk,
             "h2d": (A.numel() + B.numel()) * 8, "d2h": O.numel() * 8, "L": L, "K": K, "e2e_chunks": CH,
-            "int_ceiling": int_ceiling(lib, moduli[0]), "int_ceiling_slack": int_ceiling(lib, moduli[0], slack=True),
-            "mul64": mul64_rates(lib),
-            "slack_share": slack_shares(moduli, L, N.bit_length() - 1), "sub": SUB}
+            "int_ceiling": int_ceiling(lib, moduli[0]), "int_ceiling_slack": int_ceiling(lib, moduli[0], kind="slack"),
+            "int_ceiling_wide": int_ceiling(lib, moduli[0], kind="wide"), "mul64": mul64_rates(lib),
+            "butterfly_mix": butterfly_mix(moduli, L, N.bit_length() - 1), "sub": SUB}
 
 
 def run_ntt_sweep(batch=256, reps=10):
@@ -461,7 +461,7 @@ def run_ntt_sweep(batch=256, reps=10):
         moduli = [int(m) for m in mods]
         if ceiling is None:
             ceiling = int_ceiling(lib, moduli[0])
-            ceiling_slack = int_ceiling(lib, moduli[0], slack=True)
+            ceiling_slack = int_ceiling(lib, moduli[0], kind="slack")
         # forward: stages above 2^14 run separately (Harvey), the 2^14 blocks defer
         sh = (min(logn, 14) - fwd_subtracting_stages(min(logn, 14))) / logn
         ceilings = {"ntt_forward": 1.0 / (sh / ceiling_slack + (1.0 - sh) / ceiling), "ntt_inverse": ceiling}
@@ -807,11 +807,12 @@ def roofline(res, steps):
     ceilings = {}
     if ceil_std:
         ceilings = {k: ceil_std for k in bfly}
-        if res.get("int_ceiling_slack"):
-            # the forward transforms run the slack butterfly at most of their stages: their
-            # ceiling is the two rates weighted by their shares of the butterflies
-            for k, sh in res["slack_share"].items():
-                ceilings[k] = 1.0 / (sh / res["int_ceiling_slack"] + (1.0 - sh) / ceil_std)
+        if res.get("int_ceiling_slack") and res.get("int_ceiling_wide"):
+            # the forward transforms run three kinds of butterfly: their ceiling is the
+            # three rates weighted by the kinds' shares of their butterflies
+            rates = {"harvey": ceil_std, "slack": res["int_ceiling_slack"], "wide": res["int_ceiling_wide"]}
+            for k, mix in res["butterfly_mix"].items():
+                ceilings[k] = 1.0 / sum(sh / rates[kind] for kind, sh in mix.items())
     for k, row in table.items():
         if k in bfly and k in ceilings:
             rate = bfly[k] / (row["ms_per_step"] * 1e-3)
@@ -843,8 +844,9 @@ def roofline(res, steps):
                       "peak_source": "measured here: tb_measure_butterfly_rate, operands in registers"}
         m = res.get("mul64")
         if m:
-            # the machine bound: a butterfly's Shoup product is one high and two low 64-bit
-            # products; at the measured multiply throughputs no butterfly runs faster
+            # the machine bound of an exact-quotient butterfly: its Shoup product is one
+            # high and two low 64-bit products (the wide form estimates its quotient from
+            # 32-bit products and may pass it)
             bound = 1.0 / (1.0 / m["hi"] + 2.0 / m["lo"])
             out["int"]["machine_bound"] = {
                 "mul_lo_per_s": round(m["lo"] / 1e9, 1), "mul_hi_per_s": round(m["hi"] / 1e9, 1), "unit": "G/s",
@@ -852,12 +854,15 @@ def roofline(res, steps):
                 "ceiling_frac": round(ceil / bound, 4),
                 "source": "tb_measure_mul64_rate: mul.lo.u64 / mul.hi.u64 in independent chains; "
                           "bound = 1 / (1/hi + 2/lo) butterflies per second"}
-        if name in res.get("slack_share", {}) and res.get("int_ceiling_slack"):
+        if name in res.get("butterfly_mix", {}) and res.get("int_ceiling_wide"):
+            mix = res["butterfly_mix"][name]
             out["int"]["peak_source"] = (
                 "measured here, operands in registers: tb_measure_butterfly_rate "
-                f"({ceil_std / 1e9:.2f} G/s) and tb_measure_slack_butterfly_rate "
-                f"({res['int_ceiling_slack'] / 1e9:.2f} G/s), weighted by the share of the forward "
-                f"transform's butterflies that skip the subtraction ({res['slack_share'][name]:.4f})")
+                f"({ceil_std / 1e9:.2f} G/s), tb_measure_slack_butterfly_rate "
+                f"({res['int_ceiling_slack'] / 1e9:.2f} G/s) and tb_measure_wide_butterfly_rate "
+                f"({res['int_ceiling_wide'] / 1e9:.2f} G/s), weighted by the shares of the kernel's "
+                f"butterflies of each kind (harvey {mix['harvey']:.4f}, slack {mix['slack']:.4f}, "
+                f"wide {mix['wide']:.4f})")
     return out
 
 
@@ -871,11 +876,14 @@ def butterflies_per_step(L):
     return {k: B * v * per for k, v in limbs.items()}
 
 
-def int_ceiling(lib, q, slack=False):
+def int_ceiling(lib, q, kind="harvey"):
     """Butterflies per second of the library's lazy butterfly with everything in
     registers (tb_measure_butterfly_rate): the integer ceiling of the transforms.
-    slack: the butterfly without the conditional subtraction (tb_measure_slack_butterfly_rate)."""
-    fn = lib.tb_measure_slack_butterfly_rate if slack else lib.tb_measure_butterfly_rate
+    kind "slack": the butterfly without the conditional subtraction
+    (tb_measure_slack_butterfly_rate); "wide": the no-subtraction form's butterfly with
+    the estimated quotient (tb_measure_wide_butterfly_rate)."""
+    fn = {"harvey": lib.tb_measure_butterfly_rate, "slack": lib.tb_measure_slack_butterfly_rate,
+          "wide": lib.tb_measure_wide_butterfly_rate}[kind]
     fn.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
     r = ctypes.c_double(0)
     import tb_capi
@@ -910,27 +918,34 @@ def mul64_rates(lib):
     return out
 
 
-def slack_shares(moduli, L, logn):
-    """Per forward-transform kernel at the benchmark shape, the share of its butterflies
-    that run the slack butterfly (no subtraction). A limb of modulus q runs none of its
-    stages subtracting when q < 2^58 (in the key-switch mod-up: with at most 15 digits),
-    all but fwd_subtracting_stages(logn) of them when q < 2^60, every one otherwise. The
-    mod-up covers digit j on every key modulus but its own at L data limbs and at L-1
-    after the rescale; the mod-down and the rescale transform data limbs."""
+def butterfly_mix(moduli, L, logn):
+    """Per forward-transform kernel at the benchmark shape, the shares of its butterflies
+    of each kind: "wide" (no subtraction, estimated quotient: limbs of moduli below 2^57,
+    in the mod-up at most 15 digits), "slack" (the non-subtracting stages of the
+    deferred-reduction form, moduli below 2^60) and "harvey" (its subtracting stages,
+    and every stage above 2^60). The mod-up covers digit j on every key modulus but its
+    own at L data limbs and at L-1 after the rescale; the mod-down and the rescale
+    transform data limbs."""
     special = moduli[-1]
-    part = (logn - fwd_subtracting_stages(logn)) / logn
+    sub = fwd_subtracting_stages(logn) / logn
 
-    def share(q, wide):
-        return 1.0 if wide and q < (1 << 58) else part if q < (1 << 60) else 0.0
+    def kinds(q, wide):
+        if wide and q < (1 << 57):
+            return {"wide": 1.0, "slack": 0.0, "harvey": 0.0}
+        if q < (1 << 60):
+            return {"wide": 0.0, "slack": 1.0 - sub, "harvey": sub}
+        return {"wide": 0.0, "slack": 0.0, "harvey": 1.0}
+
+    def mean(rows):
+        return {k: sum(r[k] for r in rows) / len(rows) for k in ("wide", "slack", "harvey")}
 
     up = []
     for lv in (L, L - 1):
         targets = list(moduli[:lv]) + [special]
-        up += [share(q, lv <= 15) for j in range(lv) for i, q in enumerate(targets) if i != j]
-    down = [share(q, True) for lv in (L, L - 1) for q in moduli[:lv]]
-    resc = [share(q, True) for q in moduli[:L - 1]]
-    return {"ks_modup_ntt": sum(up) / len(up), "ks_moddown": sum(down) / len(down),
-            "rescale_ntt": sum(resc) / len(resc)}
+        up += [kinds(q, lv <= 15) for j in range(lv) for i, q in enumerate(targets) if i != j]
+    down = [kinds(q, True) for lv in (L, L - 1) for q in moduli[:lv]]
+    resc = [kinds(q, True) for q in moduli[:L - 1]]
+    return {"ks_modup_ntt": mean(up), "ks_moddown": mean(down), "rescale_ntt": mean(resc)}
 
 
 TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "ckks_step_n16384_traffic.md")

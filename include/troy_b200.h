@@ -419,10 +419,14 @@ int tb_autotune_ntt(tb_context *ctx, uint64_t polys, void *stream, int *forward_
    reference. */
 int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
 /* The same rate for the butterfly without the conditional subtraction of its first
-   input, which the key-switch mod-up transforms run for key moduli below 2^58 (their
-   consumer, the 128-bit inner product, takes the unreduced outputs). No counterpart in
-   the reference. */
+   input, which the forward transforms with deferred reductions run at most stages for
+   moduli below 2^60. No counterpart in the reference. */
 int tb_measure_slack_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
+/* The same rate for the no-subtraction form's butterfly (moduli below 2^57 in the
+   one-CTA forward transforms of the mod-up, the CKKS mod-down and the rescale), whose
+   Shoup quotient is estimated from three 32-bit partial products. No counterpart in the
+   reference. */
+int tb_measure_wide_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second);
 /* The device's 64-bit integer multiply throughput in products per second: kind 0 the
    low word (mul.lo.u64), kind 1 the high word (mul.hi.u64), each in long independent
    chains at full occupancy. A Shoup product is one high and two low products, so

@@ -131,12 +131,12 @@ struct ModUpOp {
     const uint64_t *chain;    // device copy of chain values (for the reduce test)
     int L, K, ckks, logn;
     // Up to 15 digits are summed unreduced by the 128-bit inner products: below 4q (a
-    // 61-bit q), below 16 q (q < 2^60, deferred reductions), or, for q < 2^58 in the
-    // one-CTA transform (no subtraction at all), below 2^61 + 28 q < 2^63.1: the digit
-    // then enters unreduced (below q_j < 2^61) and the transform's 14 stages add at most
-    // 2q each. 15 products below 4 q * q < 2^124, 16 q * q < 2^124 or 2^63.1 * 2^58 stay
-    // below 2^128. More digits are reduced to [0, q) at the store (the transform then
-    // stays below 16 q).
+    // 61-bit q), below 16 q (q < 2^60, deferred reductions), or, for q < 2^57 in the
+    // one-CTA transform (no subtraction, estimated quotients), below 2^61 + 56 q <
+    // 2^63.2: the digit then enters unreduced (below q_j < 2^61) and the transform's 14
+    // stages add at most 4q each. 15 products below 4 q * q < 2^124, 16 q * q < 2^124 or
+    // 2^63.2 * 2^57 stay below 2^128. More digits are reduced to [0, q) at the store (the
+    // transform then stays below 16 q).
     static constexpr int LAZY_MAX_L = 15;
     static constexpr bool wide_slack = true;
     struct Ctx {
@@ -166,7 +166,7 @@ struct ModUpOp {
         c.ratio_hi = m.ratio_hi;
         // the transform's input: any digit word in the no-subtraction form, below 4q in
         // the others (a Barrett remainder in [0, 2q) when q_j is larger)
-        const bool wide = L <= LAZY_MAX_L && logn <= MAX_LOGB && m.value < (1ull << 58);
+        const bool wide = L <= LAZY_MAX_L && logn <= MAX_LOGB && m.value < (1ull << 57);
         c.slack = wide ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         c.reduce = !wide && mods[j].value > 4 * m.value;
         c.in = src + (size_t)cb * sstride + ((size_t)j << logn);
@@ -379,7 +379,7 @@ struct ModDownBase {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)K * K + j];
         c.reduce = mods[K - 1].value > m.value;
-        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 57)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         c.wide_off = (m.ratio_hi - 1) * m.value;
         c.acc = acc + (((size_t)bc * (L + 1) + j) << logn);
         c.last = last + ((size_t)bc << logn);
@@ -403,8 +403,8 @@ struct ModDownBase {
 // (at most q_j). After the deferred-reduction form (ntt below 16 q_j) one subtraction of
 // 8 q_j brings ntt below 8 q_j and the epilogue takes acc + 8 q_j - ntt: below 9 q_j <
 // 2^64, where acc + 16 q_j - ntt would pass 2^64 for a 60-bit q_j. The no-subtraction
-// form (q_j < 2^58, one CTA per limb) takes r itself (below 2^61) plus fix: ntt stays
-// below 2^61 + 29 q_j < 2^63.3 < 2^64 - 2 q_j <= wide_off, and the epilogue takes
+// form (q_j < 2^57, one CTA per limb) takes r itself (below 2^61) plus fix: ntt stays
+// below 2^61 + 57 q_j < 2^63.2 < 2^64 - 2 q_j <= wide_off, and the epilogue takes
 // acc + wide_off - ntt, below 2^64. The same residue each way.
 struct ModDownCkksOp : ModDownBase {
     __device__ Ctx ctx(int b) const { return make(b); }

@@ -87,6 +87,23 @@ __device__ __forceinline__ void ct_butterfly_sub(uint64_t &x, uint64_t &y, ulong
     y = u + q2 - v;
 }
 
+// The no-subtraction form's butterfly (q < 2^57): the Shoup quotient floor(y wq / 2^64)
+// estimated from three 32-bit partial products, y1 w1 + hi(y1 w0) + hi(y0 w1), which
+// drops y0 w0 and two carries: at most 2 below the exact quotient for any 64-bit y, so
+// the product lies in [0, 4q) and x grows by at most 4q a stage (y stays below x's
+// bound + 4q).
+__device__ __forceinline__ uint64_t mul_shoup_lazy4(uint64_t y, uint64_t w, uint64_t wq, uint64_t q) {
+    const uint32_t y0 = (uint32_t)y, y1 = (uint32_t)(y >> 32), w0 = (uint32_t)wq, w1 = (uint32_t)(wq >> 32);
+    const uint64_t qt = (uint64_t)y1 * w1 + __umulhi(y1, w0) + __umulhi(y0, w1);
+    return w * y - qt * q;
+}
+
+__device__ __forceinline__ void ct_butterfly_wide(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q4) {
+    const uint64_t v = mul_shoup_lazy4(y, w.x, w.y, q);
+    y = x + q4 - v;
+    x = x + v;
+}
+
 // Forward stages with deferred reductions, bound M (in multiples of q). Values entering
 // local stage k of a transform from inputs below 4q stay below fwd_bound(M, k) q: a stage
 // skips the subtraction (bound + 2q) unless that would pass M q; then it first subtracts
@@ -103,14 +120,15 @@ __host__ __device__ constexpr bool fwd_subtracts(int M, int k) { return fwd_boun
 static_assert(fwd_bound(4, 14) == 4 && fwd_subtracts(4, 0) && fwd_subtracts(4, 13), "Harvey stages");
 static_assert(fwd_bound(16, 17) <= 16 && !fwd_subtracts(16, 5) && fwd_subtracts(16, 6) && fwd_subtracts(16, 10),
               "deferred stages");
-static_assert(fwd_bound(64, 17) == 38 && !fwd_subtracts(64, 16), "no subtraction below 2^58");
+static_assert(!fwd_subtracts(64, 16), "no subtraction in the wide form");
 
 // An Op context with an int member `slack` selects per CTA the bound M of its forward
 // transform: 0 for the Harvey stages, SLACK_M (q < 2^60: outputs below 16 q) or, for an
-// Op that declares `static constexpr bool wide_slack = true`, SLACK_WIDE (q < 2^58: no
-// subtraction at all, outputs below (4 + 2 log2 N) q <= 38 q). The Op takes those
-// outputs at its store. The CTA-pair and cluster forms always run the Harvey stages
-// (outputs below 4q).
+// Op that declares `static constexpr bool wide_slack = true`, SLACK_WIDE (q < 2^57, one
+// CTA per limb: no subtraction at all and the estimated quotient, ct_butterfly_wide;
+// from inputs below B the outputs stay below B + 4 q log2 N, below 2^61 + 56 q < 2^63.2
+// for inputs below 2^61 at N <= 16384). The Op takes those outputs at its store. The
+// CTA-pair and cluster forms always run the Harvey stages (outputs below 4q).
 constexpr int SLACK_M = 16;
 constexpr int SLACK_WIDE = 64;
 template <class Ctx, class = void>
@@ -182,7 +200,7 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
     constexpr int GR = SIDE ? IT : 1;                // groups in flight at once
     constexpr bool FULL = G > 0 && G % T == 0;
     constexpr int logsub = LOGB - s - R_LOG;
-    const uint64_t q = c.lm.q, q2 = q << 1, qs = q * (uint64_t)(M / 2);
+    const uint64_t q = c.lm.q, q2 = q << 1, qs = q * (uint64_t)(M / 2), q4 = q << 2;
 #pragma unroll
     for (int i0 = 0; i0 < IT; i0 += GR) {
         uint64_t v[GR][R];
@@ -210,7 +228,9 @@ __device__ __forceinline__ void fwd_pass(const Op &op, const Ctx &c, uint64_t *s
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     if (k & half) continue;
-                    if (fwd_subtracts(M, s + t))
+                    if constexpr (M == SLACK_WIDE)
+                        ct_butterfly_wide(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q4);
+                    else if (fwd_subtracts(M, s + t))
                         ct_butterfly_sub(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2, qs);
                     else
                         ct_butterfly_slack(v[it][k], v[it][k + half], __ldg(row + (k >> (R_LOG - t))), q, q2);

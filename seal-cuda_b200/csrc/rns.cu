@@ -118,7 +118,7 @@ struct RescaleNttOp {
         c.ratio_hi = m.ratio_hi;
         c.d = drop[(size_t)L * K + j];
         c.reduce = mods[L - 1].value > m.value;
-        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 58)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
+        c.slack = (logn <= MAX_LOGB && m.value < (1ull << 57)) ? SLACK_WIDE : m.value < (1ull << 60) ? SLACK_M : 0;
         c.wide_off = (m.ratio_hi - 1) * m.value;
         const size_t cb = p / size, k = p % size;
         c.in = in + cb * istride + ((k * L + j) << logn);
@@ -127,7 +127,7 @@ struct RescaleNttOp {
         return c;
     }
     // the transform takes any input below 4 q_j: the Barrett remainder (< 2 q_j) plus fix
-    // (at most q_j); the no-subtraction form (q_j < 2^58, one CTA per limb) takes r itself
+    // (at most q_j); the no-subtraction form (q_j < 2^57, one CTA per limb) takes r itself
     // (below 2^61) plus fix
     __device__ uint64_t load(const Ctx &c, int e) const {
         uint64_t x = c.r[e];
@@ -143,7 +143,7 @@ struct RescaleNttOp {
         const uint64_t q = c.lm.q;
         // after deferred reductions v is below 16 q: one subtraction of 8 q keeps
         // in + 8 q - v below 9 q < 2^64 (in + 16 q - v would pass 2^64 for a 60-bit q);
-        // after the no-subtraction form v is below 2^61 + 29 q < 2^63.3 < wide_off, and
+        // after the no-subtraction form v is below 2^61 + 57 q < 2^63.2 < wide_off, and
         // in + wide_off - v stays below 2^64
         const uint64_t x = c.slack == SLACK_WIDE ? in + c.wide_off - v
                            : c.slack ? in + (q << 3) - csub(v, q << 3) : in + (q << 2) - v;

@@ -126,21 +126,24 @@ int autotune_ntt(Context &c, uint64_t polys, cudaStream_t s, int *chosen_fwd, in
 // (ct_butterfly, the one every forward NTT pass runs) with its operands and twiddles in
 // registers, so that nothing but the 64-bit modular arithmetic is timed. Each thread
 // runs the three stages of a radix-8 group (12 butterflies, 7 twiddles) `rounds` times
-// over values kept in [0, 4q); the grid fills every SM at full occupancy. SLACK times
-// ct_butterfly_slack instead (the forward transforms of the key-switch mod-up for key
-// moduli below 2^58); its values wrap modulo 2^64 over the rounds, which changes no
+// over values kept in [0, 4q); the grid fills every SM at full occupancy. KIND 1 times
+// ct_butterfly_slack (the deferred-reduction stages of moduli below 2^60) and KIND 2
+// ct_butterfly_wide (the no-subtraction form with estimated quotients, moduli below
+// 2^57) instead; their values wrap modulo 2^64 over the rounds, which changes no
 // instruction and so not the rate.
 struct Twiddles7 {
     ulonglong2 w[7];
 };
 
-template <bool SLACK>
+// KIND 0: ct_butterfly (Harvey); 1: ct_butterfly_slack; 2: ct_butterfly_wide
+template <int KIND>
 __device__ __forceinline__ void rate_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
-    if constexpr (SLACK) ct_butterfly_slack(x, y, w, q, q2);
+    if constexpr (KIND == 2) ct_butterfly_wide(x, y, w, q, q2 << 1);
+    else if constexpr (KIND == 1) ct_butterfly_slack(x, y, w, q, q2);
     else ct_butterfly(x, y, w, q, q2);
 }
 
-template <bool SLACK>
+template <int KIND>
 __global__ void __launch_bounds__(256) butterfly_rate_kernel(uint64_t *sink, Twiddles7 tw, uint64_t q, int rounds) {
     const uint64_t q2 = q << 1;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -149,12 +152,12 @@ __global__ void __launch_bounds__(256) butterfly_rate_kernel(uint64_t *sink, Twi
     for (int k = 0; k < 8; k++) v[k] = (tid * 8u + (uint32_t)k) % q;
     for (int r = 0; r < rounds; r++) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) rate_butterfly<SLACK>(v[k], v[k + 4], tw.w[0], q, q2);
+        for (int k = 0; k < 4; k++) rate_butterfly<KIND>(v[k], v[k + 4], tw.w[0], q, q2);
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            if (!(k & 2)) rate_butterfly<SLACK>(v[k], v[k + 2], tw.w[1 + (k >> 2)], q, q2);
+            if (!(k & 2)) rate_butterfly<KIND>(v[k], v[k + 2], tw.w[1 + (k >> 2)], q, q2);
 #pragma unroll
-        for (int k = 0; k < 8; k += 2) rate_butterfly<SLACK>(v[k], v[k + 1], tw.w[3 + (k >> 1)], q, q2);
+        for (int k = 0; k < 8; k += 2) rate_butterfly<KIND>(v[k], v[k + 1], tw.w[3 + (k >> 1)], q, q2);
     }
     uint64_t x = 0;
 #pragma unroll
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(256) butterfly_rate_kernel(uint64_t *sink, Twi
     sink[tid] = x;
 }
 
-int measure_butterfly_rate(uint64_t q, bool slack, cudaStream_t s, double *rate) {
+int measure_butterfly_rate(uint64_t q, int kind, cudaStream_t s, double *rate) {
     if (!rate || q < 3 || !(q & 1) || q >= (1ull << 61))
         return set_error(TB_ERR_INVALID_ARGUMENT, "modulus must be odd, at least 3 and below 2^61");
     Twiddles7 tw;
@@ -175,7 +178,7 @@ int measure_butterfly_rate(uint64_t q, bool slack, cudaStream_t s, double *rate)
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const auto kernel = slack ? butterfly_rate_kernel<true> : butterfly_rate_kernel<false>;
+    const auto kernel = kind == 2 ? butterfly_rate_kernel<2> : kind == 1 ? butterfly_rate_kernel<1> : butterfly_rate_kernel<0>;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
     if (e != cudaSuccess) return status_from(e);
     const unsigned blocks = (unsigned)(sms * std::max(per_sm, 1));
@@ -264,11 +267,15 @@ int tb_measure_mul64_rate(int kind, void *stream, double *products_per_second) {
 
 
 int tb_measure_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second) {
-    return tb::measure_butterfly_rate(modulus, false, (cudaStream_t)stream, butterflies_per_second);
+    return tb::measure_butterfly_rate(modulus, 0, (cudaStream_t)stream, butterflies_per_second);
 }
 
 int tb_measure_slack_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second) {
-    return tb::measure_butterfly_rate(modulus, true, (cudaStream_t)stream, butterflies_per_second);
+    return tb::measure_butterfly_rate(modulus, 1, (cudaStream_t)stream, butterflies_per_second);
+}
+
+int tb_measure_wide_butterfly_rate(uint64_t modulus, void *stream, double *butterflies_per_second) {
+    return tb::measure_butterfly_rate(modulus, 2, (cudaStream_t)stream, butterflies_per_second);
 }
 
 int tb_ntt_set_variant(int forward, int log_block, int variant) {

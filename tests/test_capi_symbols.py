@@ -41,7 +41,7 @@ def test_misaligned_buffers_and_odd_strides_are_refused_on_the_host():
 
 def test_butterfly_rate_refuses_bad_moduli_on_the_host():
     lib = tb_capi.lib()
-    for fn in (lib.tb_measure_butterfly_rate, lib.tb_measure_slack_butterfly_rate):
+    for fn in (lib.tb_measure_butterfly_rate, lib.tb_measure_slack_butterfly_rate, lib.tb_measure_wide_butterfly_rate):
         fn.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         r = ctypes.c_double(0)
         for q in (0, 2, 1 << 40, (1 << 61) + 1):

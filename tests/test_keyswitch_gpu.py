@@ -237,16 +237,17 @@ def test_persistent_keyswitch_matches_oracle(orc, scheme, n, bits, t):
 
 @pytest.mark.parametrize("scheme", [CKKS, BFV])
 def test_keyswitch_slack_bounds(orc, scheme):
-    """The mod-up transforms of key moduli below 2^58 skip the butterflies' conditional
-    subtraction and hand the inner product values below (4 + 2 log2 N) q. Worst case of
-    that bound: N = 16384, 58-bit data primes (the largest that take the slack path)
-    with random residues (products near q^2), 15 digits (the most summed unreduced),
-    and 16 digits, where the digits are reduced before the sum; a 60-bit special prime
-    runs the usual butterfly in the same launch. Bit-exact against the oracle."""
+    """The mod-up transforms defer their reductions and hand the inner product unreduced
+    digits: key moduli below 2^57 run no subtraction with estimated quotients (digits
+    below 2^61 + 56 q), those below 2^60 subtract at two stages (digits below 16 q).
+    Worst cases of those bounds: N = 16384, 57-bit and 58-bit data primes (the largest of
+    each form) with random residues near q (products near q^2), 15 digits (the most
+    summed unreduced) and 16 digits, where the digits are reduced before the sum; a 60-bit
+    special prime in the same launches. Bit-exact against the oracle."""
     n = 16384
     logn = n.bit_length() - 1
-    moduli = orc.coeff_modulus_create(n, [58] * 16 + [60])
-    assert all(q < (1 << 58) for q in moduli[:-1]) and moduli[-1] >= (1 << 58)
+    moduli = orc.coeff_modulus_create(n, [57] * 8 + [58] * 8 + [60])
+    assert all(q < (1 << 57) for q in moduli[:8]) and all((1 << 57) <= q < (1 << 58) for q in moduli[8:16])
     t = 0 if scheme == CKKS else orc.plain_modulus_batching(n, 20)
     ctx = tb_capi.Context(scheme, n, moduli, t)
     K = len(moduli)
@@ -266,8 +267,8 @@ def test_keyswitch_slack_bounds(orc, scheme):
 
 
 def test_wide_form_takes_unreduced_inputs(orc):
-    """Limbs of moduli below 2^58 run the one-CTA forward transforms with no subtraction
-    and take their inputs unreduced: the mod-up the digit of a larger modulus, the CKKS
+    """Limbs of moduli below 2^57 run the one-CTA forward transforms with no subtraction
+    (estimated quotients) and take their inputs unreduced: the mod-up the digit of a larger modulus, the CKKS
     mod-down and rescale the 60-bit residue being dropped. Chain {57, 57, 60} + a 60-bit
     special prime at N = 16384: key switching (60-bit digit into 57-bit moduli, special
     residue into 57-bit limbs) and rescaling (the 60-bit last limb into 57-bit limbs),
@@ -275,7 +276,7 @@ def test_wide_form_takes_unreduced_inputs(orc):
     n = 16384
     logn = n.bit_length() - 1
     moduli = orc.coeff_modulus_create(n, [57, 57, 60, 60])
-    assert moduli[0] < (1 << 58) and moduli[2] >= (1 << 59)
+    assert moduli[0] < (1 << 57) and moduli[2] >= (1 << 59)
     ctx = tb_capi.Context(CKKS, n, moduli, 0)
     K, L = len(moduli), len(moduli) - 1
     rng = np.random.default_rng(57)
