@@ -7,13 +7,17 @@
 // ciphertexts goes through five launches:
 //   1. (CKKS) inverse NTT of every target limb;
 //   2. mod-up: one fused forward-NTT CTA per (ciphertext, digit j, key modulus i)
-//      whose load reduces digit j mod q_i;
-//   3. inner product of the digits with both key components (lazy 128-bit sums);
-//   4. inverse NTT of the special-prime accumulators with the rounding offset;
+//      that takes digit j into key modulus i (unreduced, or reduced in its load) and
+//      stores the transform's unreduced outputs;
+//   3. inner product of the digits with both key components (lazy 128-bit sums) for
+//      the data moduli;
+//   4. inverse NTT of the special-prime accumulators, whose load runs the special
+//      modulus's inner product, with the rounding offset;
 //   5. mod-down: one fused NTT (CKKS) or inverse NTT (BFV/BGV) CTA per output limb
 //      whose epilogue subtracts the special-prime part, scales by q_k^-1 and adds
 //      into the ciphertext.
-// All values are exact residues, so the result is word-identical to the reference.
+// Only exact residues matter between the steps, so the result is word-identical to
+// the reference.
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -118,11 +122,11 @@ struct StridedNttOp {
     }
 };
 
-// Step 2: forward NTT of digit j (coefficient form) reduced into key modulus i.
-// Only exact residues matter downstream (the inner product reduces its 128-bit sums),
-// so the load leaves its Barrett remainder in [0, 2q) (the transform takes inputs
-// below 4q) and, while the sums stay below 2^128, the store keeps the transform's lazy
-// [0, 4q) outputs: products below 4q * q < 2^124 (q < 2^61), at most 15 of them.
+// Step 2: forward NTT of digit j (coefficient form) into key modulus i. Only exact
+// residues matter downstream (the inner product reduces its 128-bit sums), so the
+// transform defers its reductions (ntt.cuh), takes the digit unreduced where its bound
+// allows (or a Barrett remainder in [0, 2q)), and, while the sums stay below 2^128,
+// the store keeps its unreduced outputs (bounds below).
 struct ModUpOp {
     const uint64_t *src;      // CKKS: inverse-transformed targets [B][L][N]; else targets
     uint64_t sstride;         // words between ciphertexts in src
@@ -219,7 +223,7 @@ __device__ __forceinline__ void ks_inner_pair(const uint64_t *__restrict__ digit
 
 constexpr int INNER_THREADS = 128;
 
-__global__ void ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
+__global__ void __launch_bounds__(INNER_THREADS, 8) ks_inner_kernel(const uint64_t *__restrict__ digits, const uint64_t *__restrict__ target,
                                 uint64_t tstride, KeyGroups keys, uint64_t *__restrict__ acc,
                                 const Mod *__restrict__ mods, int L, int K, int ckks, int logn) {
     const uint32_t e = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
