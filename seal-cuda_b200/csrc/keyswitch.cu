@@ -97,11 +97,13 @@ struct StridedNttOp {
         NttLimb lm;
         const uint64_t *in;
         uint64_t *out;
+        int islack;   // full inverse outputs: the wide inverse form (outputs below 4q)
     };
     __device__ Ctx ctx(int b) const {
         const int p = b / limbs, l = b % limbs;
         Ctx c;
         c.lm = make_limb(mods[first + l], 0);
+        c.islack = !FWD && !lazy;
         c.in = in + (size_t)p * istride + ((size_t)l << logn);
         c.out = out + (size_t)p * ostride + ((size_t)l << logn);
         return c;
@@ -114,7 +116,7 @@ struct StridedNttOp {
     }
     __device__ uint64_t fix(const Ctx &c, uint64_t v) const {
         if (lazy) return v;
-        return FWD ? full_fwd(v, c.lm.q) : csub(v, c.lm.q);
+        return FWD ? full_fwd(v, c.lm.q) : csub(csub(v, 2 * c.lm.q), c.lm.q);
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = fix(c, v); }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
@@ -314,6 +316,7 @@ struct SpecialInnerOp {
         const uint64_t *d, *k;
         uint64_t *out;
         uint64_t ratio_lo, ratio_hi;
+        int islack;   // the wide inverse form: outputs below 4q, reduced at the store
     };
     __device__ Ctx ctx(int b) const {
         const int cb = b >> 1, comp = b & 1;
@@ -325,6 +328,7 @@ struct SpecialInnerOp {
         c.d = digits + (((size_t)cb * L * (L + 1) + L) << logn);
         c.k = keys.of((uint32_t)cb) + (((size_t)comp * K + K - 1) << logn);
         c.out = last + ((size_t)b << logn);
+        c.islack = 1;
         return c;
     }
     __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
@@ -346,6 +350,7 @@ struct SpecialInnerOp {
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const {
         const uint64_t q = c.lm.q;
+        v = csub(v, 2 * q);   // [0, 2q) from the wide inverse form's [0, 4q)
         if (bgv) {
             c.out[e] = csub(v, q);
         } else {

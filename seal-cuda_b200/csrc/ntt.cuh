@@ -140,6 +140,22 @@ struct WideSlack : std::false_type {};
 template <class Op>
 struct WideSlack<Op, std::void_t<decltype(Op::wide_slack)>> : std::bool_constant<Op::wide_slack> {};
 
+// The inverse transform's wide form, for an Op whose context has an int member `islack`
+// set (its store reduces the outputs itself): values below 4q between stages instead of
+// 2q, the sum reduced by 4q, the difference's Shoup product with the estimated quotient
+// (mul_shoup_lazy4, [0, 4q)); the last, N^-1-scaled stage multiplies both outputs without
+// reducing the sum first. Outputs below 4q. Only whole-limb single-CTA launches run it.
+__device__ __forceinline__ void gs_butterfly_wide(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q4) {
+    const uint64_t u = x, v = y;
+    x = csub(u + v, q4);
+    y = mul_shoup_lazy4(u + q4 - v, w.x, w.y, q);
+}
+
+template <class Ctx, class = void>
+struct HasInvSlack : std::false_type {};
+template <class Ctx>
+struct HasInvSlack<Ctx, std::void_t<decltype(std::declval<Ctx>().islack)>> : std::true_type {};
+
 __device__ __forceinline__ void gs_butterfly(uint64_t &x, uint64_t &y, ulonglong2 w, uint64_t q, uint64_t q2) {
     uint64_t u = x, v = y;
     uint64_t s = u + v;
@@ -360,7 +376,8 @@ __global__ void __launch_bounds__(NttCfg<LOGB, V>::THREADS) ntt_fwd_kernel(Op op
 // Pass of R_LOG Gentleman-Sande stages starting at local stage s; global stage =
 // local stage (an inverse CTA always owns the low stages). logn is log2 of the full
 // limb length; SCALE folds N^-1 into the pass's last stage.
-template <int R_LOG, bool TO_GLOBAL, bool SCALE, int LOGB, int T, int s, bool SIDE, class Op, class Ctx>
+template <int R_LOG, bool TO_GLOBAL, bool SCALE, int LOGB, int T, int s, bool SIDE, bool W = false, class Op,
+          class Ctx>
 __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *sm, int logn) {
     constexpr int R = 1 << R_LOG;
     constexpr int NB = 1 << LOGB;
@@ -368,7 +385,7 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
     constexpr int IT = G > 0 ? (G + T - 1) / T : 1;  // groups per thread
     constexpr int GR = SIDE ? IT : 1;                // groups in flight at once
     constexpr bool FULL = G > 0 && G % T == 0;
-    const uint64_t q = c.lm.q, q2 = q << 1;
+    const uint64_t q = c.lm.q, q2 = q << 1, q4 = q << 2;
     const uint32_t n = 1u << logn;
 #pragma unroll
     for (int i0 = 0; i0 < IT; i0 += GR) {
@@ -395,7 +412,13 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     if (k & h) continue;
-                    if (SCALE && t == R_LOG - 1) {
+                    if (W && SCALE && t == R_LOG - 1) {
+                        const uint64_t u = v[it][k], y = v[it][k + h];
+                        v[it][k] = mul_shoup_lazy4(u + y, c.lm.inv_n, c.lm.inv_n_quo, q);
+                        v[it][k + h] = mul_shoup_lazy4(u + q4 - y, c.lm.sroot, c.lm.sroot_quo, q);
+                    } else if (W) {
+                        gs_butterfly_wide(v[it][k], v[it][k + h], __ldg(c.lm.iroots + rb + (k >> (t + 1))), q, q4);
+                    } else if (SCALE && t == R_LOG - 1) {
                         uint64_t u = csub(v[it][k], q2);
                         uint64_t y = v[it][k + h];
                         uint64_t sum = u + y;
@@ -434,11 +457,11 @@ __device__ __forceinline__ void inv_pass(const Op &op, const Ctx &c, uint64_t *s
 }
 
 // Radix-8 passes P .. PASSES-1 (local stages 3P ..), unrolled at compile time.
-template <int P, int PASSES, int LOGB, int T, bool SIDE, class Op, class Ctx>
+template <int P, int PASSES, int LOGB, int T, bool SIDE, bool W = false, class Op, class Ctx>
 __device__ __forceinline__ void inv_passes(const Op &op, const Ctx &c, uint64_t *sm, int logn) {
     if constexpr (P < PASSES) {
-        inv_pass<3, false, false, LOGB, T, 3 * P, SIDE>(op, c, sm, logn);
-        inv_passes<P + 1, PASSES, LOGB, T, SIDE>(op, c, sm, logn);
+        inv_pass<3, false, false, LOGB, T, 3 * P, SIDE, W>(op, c, sm, logn);
+        inv_passes<P + 1, PASSES, LOGB, T, SIDE, W>(op, c, sm, logn);
     }
 }
 
@@ -482,6 +505,13 @@ __device__ __forceinline__ void ntt_inv_limb(const Op &op, int limb, int logn, i
     inv_copy_in<LOGB, T>(op, c, sm, 0);
     constexpr int LAST = REM ? REM : 3;
     constexpr int PASSES = REM ? LOGB / 3 : LOGB / 3 - 1;  // radix-8 passes before the last one
+    if constexpr (HasInvSlack<decltype(c)>::value) {
+        if (c.islack && scale_last) {
+            inv_passes<0, PASSES, LOGB, T, false, true>(op, c, sm, logn);
+            inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, false, true>(op, c, sm, logn);
+            return;
+        }
+    }
     inv_passes<0, PASSES, LOGB, T, false>(op, c, sm, logn);
     if (scale_last) inv_pass<LAST, true, true, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);
     else inv_pass<LAST, true, false, LOGB, T, 3 * PASSES, false>(op, c, sm, logn);

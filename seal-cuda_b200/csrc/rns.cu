@@ -67,12 +67,14 @@ struct LastInttOp {
         NttLimb lm;
         const uint64_t *in;
         uint64_t *out;
+        int islack;   // the wide inverse form: outputs below 4q, reduced at the store
     };
     __device__ Ctx ctx(int b) const {
         Ctx c;
         c.lm = make_limb(mods[L - 1], 0);
         c.in = in + (size_t)(b / size) * istride + ((size_t)((b % size) * L + L - 1) << logn);
         c.out = r + ((size_t)b << logn);
+        c.islack = 1;
         return c;
     }
     __device__ void load2(const Ctx &c, int e, uint64_t &a, uint64_t &b) const {
@@ -82,7 +84,7 @@ struct LastInttOp {
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const {
         const uint64_t q = c.lm.q;
-        v = csub(v, q);                   // canonical inverse transform
+        v = csub(csub(v, 2 * q), q);      // canonical inverse transform (from below 4q)
         uint64_t x = v + (q >> 1);
         c.out[e] = x >= q ? x - q : x;
     }
