@@ -165,7 +165,8 @@ struct PlainNttOp {
         NttLimb lm;
         const uint64_t *in;
         uint64_t *out;
-        int slack;   // full forward outputs: deferred reductions, outputs below 16 q
+        int slack;    // full forward outputs: deferred reductions, outputs below 16 q
+        int islack;   // full inverse outputs: the wide inverse form, outputs below 4q
     };
     __device__ Ctx ctx(int b) const {
         const int limb_block = b >> log_nsub;
@@ -174,6 +175,7 @@ struct PlainNttOp {
         Ctx c;
         c.lm = make_limb(mods[first + l], sb);
         c.slack = (FWD && !lazy && c.lm.q < (1ull << 60)) ? SLACK_M : 0;
+        c.islack = !FWD && !lazy;
         const size_t off = ((size_t)limb_block << (logb + log_nsub)) + ((size_t)sb << logb);
         c.in = in + off;
         c.out = out + off;
@@ -188,11 +190,8 @@ struct PlainNttOp {
     __device__ uint64_t fix(const Ctx &c, uint64_t v) const {
         if (lazy) return v;
         const uint64_t q = c.lm.q;
-        if (FWD) {
-            if (c.slack) v = csub(csub(v, 8 * q), 4 * q);
-            v = csub(v, 2 * q);
-        }
-        return csub(v, q);
+        if (FWD && c.slack) v = csub(csub(v, 8 * q), 4 * q);
+        return csub(csub(v, 2 * q), q);
     }
     __device__ void store(const Ctx &c, int e, uint64_t v) const { c.out[e] = fix(c, v); }
     __device__ void store2(const Ctx &c, int e, uint64_t a, uint64_t b) const {
