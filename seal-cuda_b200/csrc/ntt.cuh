@@ -7,11 +7,13 @@
 // stages in registers with Shoup twiddles, and writes them back; the shared-memory
 // slot of coefficient e is swz(e), which keeps every pass bank-conflict free.
 //
-// The butterflies and lazy ranges are those of the reference's DWTHandler
-// (src/utils/dwthandler.h:88-372, src/utils/ntt.h:17-60), so full and lazy
-// outputs are bit-identical to nttNegacyclicHarvey[Lazy] /
-// inverseNttNegacyclicHarvey[Lazy] (src/utils/ntt.cpp:158-213); the N^-1 scaling is
-// folded into the last inverse stage exactly as there.
+// Transforms with lazy outputs run the butterflies and lazy ranges of the reference's
+// DWTHandler (src/utils/dwthandler.h:88-372, src/utils/ntt.h:17-60), so their outputs
+// are bit-identical to nttNegacyclicHarveyLazy / inverseNttNegacyclicHarveyLazy
+// (src/utils/ntt.cpp:158-213); the N^-1 scaling is folded into the last inverse stage
+// exactly as there. Transforms whose outputs are reduced afterwards (full outputs, the
+// fused key-switch, rescale and multiply steps) may defer their reductions (the wide
+// forms below): the residues, and so the reduced outputs, are the same.
 //
 // Each kernel is parameterised by an operation `Op` that maps a CTA to its limb
 // (pointers + modulus) and supplies the global-memory load of the first pass and
