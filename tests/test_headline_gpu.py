@@ -3,7 +3,7 @@ word against the reference.
 
 Workload: CKKS, N = 16384, chain {60, 40 x 7, 60}, scale 2^40, 64 ciphertext pairs
 through multiply -> relinearize -> rescale_to_next -> rotate_vector over 13 Galois
-keys (k = 1, 2, 4, ..., 4096), as four concurrent sub-batches on four streams with the
+keys (k = 1, 2, 4, ..., 4096), as two concurrent sub-batches on two streams with the
 pairs of each step grouped into one tb_apply_galois_groups call per sub-batch
 (seal-cuda_b200/python/ckks_step.py, the class bench.py times).
 
@@ -32,7 +32,7 @@ SEEDP = (ctypes.c_uint64 * 8)(*[int(x) for x in SEED])
 N = 16384
 BITS = [60] + [40] * 7 + [60]
 PAIRS = 64
-SUB = 4
+SUB = 2   # bench.py's HEADLINE_SUB_BATCHES
 STEPS_K = [1 << i for i in range(13)]
 SCALE = 2.0 ** 40
 
@@ -87,7 +87,7 @@ def test_benchmark_step_matches_reference_words_and_decodes():
         A[i] = R.ct(ia[-1])["data"].reshape(2, L, N)
         B[i] = R.ct(ib[-1])["data"].reshape(2, L, N)
 
-    # the benchmark's step: four sub-batches on four streams
+    # the benchmark's step: two sub-batches on two streams
     step = BatchedCkksStep(torch, ctx, L, N, PAIRS, rlk, elts, gks, SUB)
     dA, dB = _dev(A), _dev(B)
     out = _empty(PAIRS, 2, L - 1, N)
