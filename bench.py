@@ -72,7 +72,7 @@ METRIC = "HE mul+relin+rescale+rotate ops/s (CKKS N=16384, batched 64 pairs)"
 WORKLOAD = "ckks_n16384_L8_batch64_mul_relin_rescale_rotate"
 FALLBACK_HBM_GBS = 6650.0
 PER_OP_PAIRS = 16
-E2E_CHUNKS = 4   # sub-batches per step in the end-to-end copy pipeline
+E2E_CHUNKS = 2   # sub-batches per step in the end-to-end copy pipeline
 HEADLINE_SUB_BATCHES = 2   # concurrent sub-batches (one stream each) per step of `value`
 # serving workload: encrypted vector x plaintext matrix (MatmulHelper coefficient
 # encoding), BFV N = 8192, 5 primes, 20-bit batching t, Poisson arrivals
@@ -311,11 +311,12 @@ def run_b200(args, rank, world):
 
     # End to end through the C ABI with host buffers: every step copies its inputs in
     # from page-locked host memory and its results back out. Each step's batch runs as
-    # E2E_CHUNKS sub-batches, the unit of the copy pipeline: the copies run on their own
+    # --e2e-chunks sub-batches, the unit of the copy pipeline: the copies run on their own
     # streams (one per direction) with two device buffer sets, so a sub-batch's inputs
     # arrive while the one before computes and the one before that leaves; events order
     # each buffer's reuse. Every pair keeps the rotation step of the batched path.
-    CH = E2E_CHUNKS if PAIRS % E2E_CHUNKS == 0 and PAIRS // E2E_CHUNKS >= len(STEPS_K) else 1
+    ech = args.e2e_chunks
+    CH = ech if ech >= 1 and PAIRS % ech == 0 and PAIRS // ech >= len(STEPS_K) else 1
     PC = PAIRS // CH
     chunk_runs = [stepper.runs(c * PC, PC) for c in range(CH)]
 
@@ -336,7 +337,9 @@ def run_b200(args, rank, world):
     # two compute streams: unit u computes on s_comp[u % 2] (with the step's scratch rows
     # of that stream), so one chunk's short launches overlap the next chunk's, as the
     # sub-batches of the step do; its buffers are set u % NBUF
-    s_comp = [torch.cuda.Stream(), torch.cuda.Stream()]
+    # (one compute stream when the step's scratch rows cannot hold two chunks)
+    NCS = 2 if 2 * PC <= PAIRS else 1
+    s_comp = [torch.cuda.Stream() for _ in range(NCS)]
     ev = lambda: torch.cuda.Event()
     pending = {}
 
@@ -353,7 +356,7 @@ def run_b200(args, rank, world):
     seeded = {"on": False}
 
     def e2e_unit(u, k, c):
-        j, sc = u % NBUF, u % 2
+        j, sc = u % NBUF, u % NCS
         rows = slice(c * PC, (c + 1) * PC)
         arrived, computed, left = ev(), ev(), ev()
         with torch.cuda.stream(s_in):
@@ -1089,6 +1092,8 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch measurement")
     ap.add_argument("--no-ntt-sweep", action="store_true", help="skip the raw transform sweep")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference CUDA path")
+    ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
+                    help="chunks per step of the end-to-end copy pipeline")
     ap.add_argument("--streams", type=int, default=HEADLINE_SUB_BATCHES,
                     help="concurrent sub-batches (one stream each) per step of the headline workload")
     ap.add_argument("--ks-persistent", action="store_true",
